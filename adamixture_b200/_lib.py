@@ -1,0 +1,95 @@
+"""ctypes binding of the C ABI in ``include/adamixture_b200.h``.
+
+The library is built in-tree (``python -m adamixture_b200.csrc.build``) into
+``adamixture_b200/_lib/libadamixture_b200.so``. There is no fallback: if the library is
+missing or fails to load, every call raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import threading
+from ctypes import c_double, c_int, c_int64, c_size_t, c_uint32, c_uint64, c_void_p
+from pathlib import Path
+
+LIB_PATH = Path(__file__).resolve().parent / "_lib" / "libadamixture_b200.so"
+
+ADX_OK, ADX_ERR_ARG, ADX_ERR_CUDA, ADX_ERR_WORKSPACE, ADX_ERR_UNSUPPORTED = 0, 1, 2, 3, 4
+ADX_F64, ADX_F32, ADX_BF16 = 0, 1, 2
+MAX_K = 64
+
+P = c_void_p
+I64 = c_int64
+
+# name -> argtypes (restype is int unless listed in _RESTYPE)
+SIGNATURES: dict[str, list] = {
+    "adx_version": [],
+    "adx_last_error": [],
+    "adx_unpack_u8": [P, I64, I64, I64, I64, I64, I64, P, P],
+    "adx_unpack_center_f32": [P, I64, I64, I64, I64, I64, I64, P, P, P],
+    "adx_allele_frequency": [P, I64, I64, P, P],
+    "adx_sample_counts": [P, I64, I64, P, P],
+    "adx_bed_workspace_bytes": [I64, I64, P],
+    "adx_bed_to_packed": [P, I64, I64, P, P, P, c_size_t, P],
+    "adx_simulate_packed": [P, P, I64, I64, c_int, c_uint64, c_uint64, c_uint32, P, P],
+    "adx_em_workspace_bytes": [I64, I64, c_int, c_int, P],
+    "adx_em_stats": [P, I64, I64, c_int, c_int, P, P, P, P, P, P, c_size_t, P],
+    "adx_em_sweep": [P, I64, I64, c_int, c_int, P, P, P, c_size_t, P],
+    "adx_em_targets": [P, P, P, P, P, P, I64, I64, c_int, P, P, P],
+    "adx_adam_step": [P, P, P, P, P, P, P, P, I64, I64, c_int, c_double, c_double, c_double,
+                      c_double, c_double, P, P, P],
+    "adx_em_adam_iteration": [P, I64, I64, c_int, c_int, P, P, P, P, P, P, P, P, P, c_double,
+                              c_double, c_double, c_double, c_double, P, c_size_t, P],
+    "adx_loglik_workspace_bytes": [I64, I64, c_int, c_int, P],
+    "adx_loglik": [P, I64, I64, c_int, c_int, P, P, P, P, c_size_t, P],
+}
+_RESTYPE = {"adx_version": ctypes.c_char_p, "adx_last_error": ctypes.c_char_p}
+
+_lock = threading.Lock()
+_lib: ctypes.CDLL | None = None
+
+
+class AdxError(RuntimeError):
+    """A library call returned an error status."""
+
+
+def load() -> ctypes.CDLL:
+    """Load the library (once) and declare every entry point's signature."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    with _lock:
+        if _lib is not None:
+            return _lib
+        if not LIB_PATH.exists():
+            raise AdxError(
+                f"{LIB_PATH} is missing; build it with `python -m adamixture_b200.csrc.build`"
+            )
+        lib = ctypes.CDLL(str(LIB_PATH))
+        for name, args in SIGNATURES.items():
+            fn = getattr(lib, name)
+            fn.argtypes = args
+            fn.restype = _RESTYPE.get(name, c_int)
+        _lib = lib
+        return lib
+
+
+def call(name: str, *args) -> None:
+    """Call entry point ``name``; raise AdxError with the library's message on failure."""
+    lib = load()
+    rc = getattr(lib, name)(*args)
+    if rc != ADX_OK:
+        msg = lib.adx_last_error().decode(errors="replace")
+        kind = {ADX_ERR_ARG: "invalid argument", ADX_ERR_CUDA: "CUDA error",
+                ADX_ERR_WORKSPACE: "workspace too small",
+                ADX_ERR_UNSUPPORTED: "unsupported"}.get(rc, f"status {rc}")
+        raise AdxError(f"{name}: {kind}: {msg}")
+
+
+def query_size(name: str, *args) -> int:
+    out = c_size_t(0)
+    call(name, *args, ctypes.addressof(out))
+    return int(out.value)
+
+
+def version() -> str:
+    return load().adx_version().decode()

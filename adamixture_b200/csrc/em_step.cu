@@ -1,0 +1,568 @@
+// Fused Adam-EM E-step for the ADMIXTURE binomial model on B200 (sm_100a), CUDA-core form.
+//
+// One sweep over the packed genotype matrix computes, for every entry (SNP j, sample i),
+//   h = P_j . Q_i,  rec = clamp(h, 1e-5, 1-1e-5),  a = g/rec,  b = (2-g)/(1-rec)  (0 if missing)
+// and accumulates both sides of the two-sided reduction
+//   A_j = sum_i a Q_i,  B_j = sum_i b Q_i           (P side: reduce over samples)
+//   T_i = sum_j (a-b) P_j + sum_j b                  (Q side: reduce over SNPs)
+// (adamixture/model/em_adam_gpu.py:46-78). The reference materialises ~6 float64 C x N
+// temporaries per 8192-SNP chunk and runs 4 DGEMMs; here G is read once, 2 bits per entry.
+//
+// Work decomposition (deterministic, no atomics):
+//  - a block owns a SNP range [j0, j1) ("SNP block", multiple of CH SNPs, quad aligned) and a
+//    residue class of sample sub-tiles ("split"); a sub-tile is TPB*SPT consecutive samples,
+//    SPT per thread (their Q rows and T accumulators live in registers);
+//  - per SNP, each thread forms its SPT samples' contributions to A_j/B_j, a warp
+//    reduce-scatter folds the 2K values over 32 lanes, a cross-warp pass folds the 8 warps
+//    and adds the block's partial into AB_part[split][j] (the block is the only writer of
+//    those rows, and always the same thread adds the same element);
+//  - after its SNP range, each thread writes T_part[snp_block][i] for its samples.
+// A second kernel reduces AB_part over splits and T_part over SNP blocks in float64, in a
+// fixed order, and either writes A/B/T or applies em_final_update + the Adam move directly.
+#include "common.cuh"
+
+#include <math.h>
+
+namespace adx {
+
+constexpr int TPB = 256;
+constexpr int WARPS = TPB / 32;
+constexpr int PLAN_BLOCKS = 592;  // target block count (4 per SM on 148 SMs); fixed so the
+                                  // partition, hence the summation order, never depends on the GPU
+
+template <typename R, int KMAX>
+struct EmCfg {
+  static constexpr int SPT = (sizeof(R) == 4) ? (KMAX <= 16 ? 4 : (KMAX <= 32 ? 2 : 1))
+                                              : (KMAX <= 8 ? 2 : 1);
+  static constexpr int W = TPB * SPT;            // samples per sub-tile
+  static constexpr int V = 2 * KMAX;             // A and B values per SNP
+  static constexpr int VP = ((V + 31) / 32) * 32;
+  static constexpr int NCH = VP / 32;
+  static constexpr int CH_RAW = 40960 / (WARPS * VP * (int)sizeof(R));
+  static constexpr int CH = CH_RAW >= 32 ? 32 : (CH_RAW / 4) * 4;  // SNPs staged per chunk
+  static_assert(CH >= 4, "chunk must hold a packed quad");
+};
+
+struct EmPlan {
+  int64_t M, N;
+  int K, kmax, prec;
+  int W, CH;
+  int64_t n_stile;   // sample sub-tiles
+  int n_split;       // sample splits (partials of A/B)
+  int n_mblk;        // SNP blocks (partials of T)
+  int64_t mb;        // SNPs per SNP block
+  size_t ab_elems, t_elems, elem_size;
+  size_t bytes() const { return (ab_elems + t_elems) * elem_size + 256; }
+};
+
+// ---------------------------------------------------------------- device helpers
+
+__device__ __forceinline__ float clampr(float x, float lo, float hi) { return fminf(fmaxf(x, lo), hi); }
+__device__ __forceinline__ double clampr(double x, double lo, double hi) { return fmin(fmax(x, lo), hi); }
+
+// a = ga/rec, b = gb/(1-rec). Float: one correctly rounded reciprocal of rec*(1-rec).
+// Double: two IEEE divisions, as the reference computes them.
+__device__ __forceinline__ void ratios(float ga, float gb, float rec, float omr, float& a, float& b) {
+  const float r = __frcp_rn(rec * omr);
+  a = ga * (omr * r);
+  b = gb * (rec * r);
+}
+__device__ __forceinline__ void ratios(double ga, double gb, double rec, double omr, double& a, double& b) {
+  a = ga / rec;
+  b = gb / omr;
+}
+
+// Warp reduce-scatter of 32 values: afterwards lane l holds sum over lanes of v[l].
+template <typename R>
+__device__ __forceinline__ R reduce_scatter32(R (&v)[32], int lane) {
+#pragma unroll
+  for (int h = 16; h >= 1; h >>= 1) {
+    const bool up = (lane & h) != 0;
+#pragma unroll
+    for (int i = 0; i < h; ++i) {
+      const R send = up ? v[i] : v[i + h];
+      const R keep = up ? v[i + h] : v[i];
+      v[i] = keep + __shfl_xor_sync(0xffffffffu, send, h);
+    }
+  }
+  return v[0];
+}
+
+// ---------------------------------------------------------------- E-step sweep
+
+template <typename R, int KMAX>
+__global__ void __launch_bounds__(TPB)
+em_sweep_kernel(const uint8_t* __restrict__ G, const R* __restrict__ P, const R* __restrict__ Q,
+                int64_t M, int64_t N, int K, int64_t n_stile, int n_split, int n_mblk, int64_t mb,
+                R* __restrict__ ABp, R* __restrict__ Tp) {
+  using C = EmCfg<R, KMAX>;
+  constexpr int SPT = C::SPT, CH = C::CH, VP = C::VP, V = C::V;
+  __shared__ R Ps[CH][KMAX];
+  __shared__ R red[WARPS][CH][VP];
+
+  const int mblk = blockIdx.x % n_mblk;
+  const int split = blockIdx.x / n_mblk;
+  const int64_t j0 = (int64_t)mblk * mb;
+  const int64_t j1 = min(M, j0 + mb);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const bool aligned4 = (SPT == 4) && ((N & 3) == 0);
+  const R ELO = (R)E_CLAMP, EHI = (R)(1.0 - E_CLAMP);
+
+  bool first = true;
+  for (int64_t st = split; st < n_stile; st += n_split) {
+    const int64_t i0 = st * C::W + (int64_t)threadIdx.x * SPT;
+    R q[SPT][KMAX], tab[SPT][KMAX], tb[SPT];
+#pragma unroll
+    for (int u = 0; u < SPT; ++u) {
+      tb[u] = 0;
+#pragma unroll
+      for (int k = 0; k < KMAX; ++k) {
+        tab[u][k] = 0;
+        q[u][k] = (i0 + u < N && k < K) ? Q[(i0 + u) * K + k] : (R)0;
+      }
+    }
+
+    for (int64_t c0 = j0; c0 < j1; c0 += CH) {
+      const int cn = (int)min((int64_t)CH, j1 - c0);
+      __syncthreads();
+      for (int e = threadIdx.x; e < CH * KMAX; e += TPB) {
+        const int jl = e / KMAX, k = e % KMAX;
+        Ps[jl][k] = (jl < cn && k < K) ? P[(c0 + jl) * K + k] : (R)0;
+      }
+      __syncthreads();
+
+      for (int qd = 0; qd < cn; qd += 4) {
+        const int64_t row = (c0 + qd) >> 2;
+        uint32_t bytes[SPT];
+        if (aligned4 && i0 < N) {
+          const uint32_t w = __ldg(reinterpret_cast<const uint32_t*>(G + row * N + i0));
+#pragma unroll
+          for (int u = 0; u < SPT; ++u) bytes[u] = (w >> (8 * u)) & 0xFFu;
+        } else {
+#pragma unroll
+          for (int u = 0; u < SPT; ++u) bytes[u] = (i0 + u < N) ? (uint32_t)__ldg(G + row * N + i0 + u) : 0xFFu;
+        }
+#pragma unroll
+        for (int s = 0; s < 4; ++s) {
+          const int jl = qd + s;
+          if (jl >= cn) break;  // uniform across the block
+          R a[SPT], b[SPT];
+#pragma unroll
+          for (int u = 0; u < SPT; ++u) {
+            const unsigned g = genotype(bytes[u], s);
+            R h = 0;
+#pragma unroll
+            for (int k = 0; k < KMAX; ++k) h += Ps[jl][k] * q[u][k];
+            const R rec = clampr(h, ELO, EHI);
+            const R omr = (R)1 - rec;
+            const R ga = (g == 3u) ? (R)0 : (R)g;
+            const R gb = (g == 3u) ? (R)0 : (R)(2u - g);
+            ratios(ga, gb, rec, omr, a[u], b[u]);
+            const R d = a[u] - b[u];
+#pragma unroll
+            for (int k = 0; k < KMAX; ++k) tab[u][k] += d * Ps[jl][k];
+            tb[u] += b[u];
+          }
+#pragma unroll
+          for (int c = 0; c < C::NCH; ++c) {
+            R part[32];
+#pragma unroll
+            for (int l = 0; l < 32; ++l) {
+              const int v = c * 32 + l;
+              R acc = 0;
+              if (v < KMAX) {
+#pragma unroll
+                for (int u = 0; u < SPT; ++u) acc += a[u] * q[u][v < KMAX ? v : 0];
+              } else if (v < V) {
+#pragma unroll
+                for (int u = 0; u < SPT; ++u) acc += b[u] * q[u][v >= KMAX && v < V ? v - KMAX : 0];
+              }
+              part[l] = acc;
+            }
+            red[warp][jl][c * 32 + lane] = reduce_scatter32(part, lane);
+          }
+        }
+      }
+      __syncthreads();
+      const int nv = cn * V;
+      for (int e = threadIdx.x; e < nv; e += TPB) {
+        const int jl = e / V, v = e % V;
+        const int k = v < KMAX ? v : v - KMAX;
+        if (k >= K) continue;
+        R sum = 0;
+#pragma unroll
+        for (int w = 0; w < WARPS; ++w) sum += red[w][jl][v];
+        R* dst = ABp + ((int64_t)split * M + (c0 + jl)) * (2 * K) + (v < KMAX ? k : K + k);
+        *dst = first ? sum : *dst + sum;
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < SPT; ++u) {
+      if (i0 + u < N) {
+        R* dst = Tp + ((int64_t)mblk * N + i0 + u) * K;
+#pragma unroll
+        for (int k = 0; k < KMAX; ++k)
+          if (k < K) dst[k] = tab[u][k] + tb[u];
+      }
+    }
+    first = false;
+  }
+}
+
+// ---------------------------------------------------------------- reduce / targets / Adam
+
+struct AdamArgs {
+  double t, lr, b1, b2, eps;
+};
+
+// mode 0: write A, B, T (float64 statistics). mode 1: EM targets + Adam move on P and Q.
+template <typename R, int KMAX>
+__global__ void em_update_kernel(const R* __restrict__ ABp, const R* __restrict__ Tp, int64_t M,
+                                 int64_t N, int K, int n_split, int n_mblk, int mode,
+                                 double* __restrict__ outA, double* __restrict__ outB,
+                                 double* __restrict__ outT, const double* __restrict__ q_bat,
+                                 double* __restrict__ P, double* __restrict__ Q,
+                                 float* __restrict__ P32, float* __restrict__ Q32,
+                                 double* __restrict__ mP, double* __restrict__ vP,
+                                 double* __restrict__ mQ, double* __restrict__ vQ, AdamArgs ad) {
+  const int64_t row = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (row >= M + N) return;
+  const double bc1 = 1.0 - pow(ad.b1, ad.t);
+  const double bc2 = 1.0 - pow(ad.b2, ad.t);
+  if (row < M) {
+    const int64_t j = row;
+    double A[KMAX], B[KMAX];
+#pragma unroll
+    for (int k = 0; k < KMAX; ++k) { A[k] = 0.0; B[k] = 0.0; }
+    for (int s = 0; s < n_split; ++s) {
+      const R* src = ABp + ((int64_t)s * M + j) * (2 * K);
+#pragma unroll
+      for (int k = 0; k < KMAX; ++k)
+        if (k < K) { A[k] += (double)src[k]; B[k] += (double)src[K + k]; }
+    }
+    if (mode == 0) {
+#pragma unroll
+      for (int k = 0; k < KMAX; ++k)
+        if (k < K) { outA[j * K + k] = A[k]; outB[j * K + k] = B[k]; }
+      return;
+    }
+#pragma unroll
+    for (int k = 0; k < KMAX; ++k) {
+      if (k >= K) continue;
+      const int64_t o = j * K + k;
+      const double p = P[o];
+      // em_final_update order: ((A-B)*P + B) -> clamp(min 1e-5) -> reciprocal -> *P -> *A
+      const double den = fmax((A[k] - B[k]) * p + B[k], 1e-5);
+      const double target = ((1.0 / den) * p) * A[k];
+      const double delta = target - p;
+      const double m = mP[o] * ad.b1 + (1.0 - ad.b1) * delta;
+      const double v = vP[o] * ad.b2 + (1.0 - ad.b2) * (delta * delta);
+      mP[o] = m;
+      vP[o] = v;
+      double np = p + (ad.lr * (m / bc1)) / (sqrt(v / bc2) + ad.eps);
+      np = fmin(fmax(np, DOMAIN), 1.0 - DOMAIN);
+      P[o] = np;
+      if (P32) P32[o] = (float)np;
+    }
+    return;
+  }
+  const int64_t i = row - M;
+  double T[KMAX];
+#pragma unroll
+  for (int k = 0; k < KMAX; ++k) T[k] = 0.0;
+  for (int b = 0; b < n_mblk; ++b) {
+    const R* src = Tp + ((int64_t)b * N + i) * K;
+#pragma unroll
+    for (int k = 0; k < KMAX; ++k)
+      if (k < K) T[k] += (double)src[k];
+  }
+  if (mode == 0) {
+#pragma unroll
+    for (int k = 0; k < KMAX; ++k)
+      if (k < K) outT[i * K + k] = T[k];
+    return;
+  }
+  const double scale = 1.0 / fmax(q_bat[i], 1e-5);
+  double qe[KMAX];
+  double s = 0.0;
+#pragma unroll
+  for (int k = 0; k < KMAX; ++k) {
+    qe[k] = (k < K) ? (Q[i * K + k] * T[k]) * scale : 0.0;
+    s += qe[k];
+  }
+  s = fmax(s, 1e-5);
+  double tot = 0.0;
+#pragma unroll
+  for (int k = 0; k < KMAX; ++k) {
+    if (k >= K) continue;
+    const int64_t o = i * K + k;
+    const double qv = Q[o];
+    const double delta = qe[k] / s - qv;
+    const double m = mQ[o] * ad.b1 + (1.0 - ad.b1) * delta;
+    const double v = vQ[o] * ad.b2 + (1.0 - ad.b2) * (delta * delta);
+    mQ[o] = m;
+    vQ[o] = v;
+    double nq = qv + (ad.lr * (m / bc1)) / (sqrt(v / bc2) + ad.eps);
+    nq = fmin(fmax(nq, DOMAIN), 1.0 - DOMAIN);
+    qe[k] = nq;
+    tot += nq;
+  }
+#pragma unroll
+  for (int k = 0; k < KMAX; ++k) {
+    if (k >= K) continue;
+    const double nq = qe[k] / tot;
+    Q[i * K + k] = nq;
+    if (Q32) Q32[i * K + k] = (float)nq;
+  }
+}
+
+// ---------------------------------------------------------------- planning and dispatch
+
+static const int KMAX_LIST[] = {2, 3, 4, 6, 8, 10, 12, 16, 24, 32, 48, 64};
+
+int pick_kmax(int K) {
+  for (int km : KMAX_LIST)
+    if (K <= km) return km;
+  return -1;
+}
+
+template <typename R, int KMAX>
+static void cfg_of(int& W, int& CH) {
+  W = EmCfg<R, KMAX>::W;
+  CH = EmCfg<R, KMAX>::CH;
+}
+
+#define ADX_KMAX_SWITCH(kmax, MACRO)                                                   \
+  switch (kmax) {                                                                      \
+    case 2: MACRO(2); break;   case 3: MACRO(3); break;   case 4: MACRO(4); break;     \
+    case 6: MACRO(6); break;   case 8: MACRO(8); break;   case 10: MACRO(10); break;   \
+    case 12: MACRO(12); break; case 16: MACRO(16); break; case 24: MACRO(24); break;   \
+    case 32: MACRO(32); break; case 48: MACRO(48); break; case 64: MACRO(64); break;   \
+    default: break;                                                                    \
+  }
+
+int em_plan(int64_t M, int64_t N, int K, int prec, EmPlan& pl) {
+  if (M <= 0 || N <= 0 || K < 1 || K > ADX_MAX_K) return ADX_ERR_ARG;
+  if (prec != ADX_F64 && prec != ADX_F32) return ADX_ERR_UNSUPPORTED;
+  pl.M = M; pl.N = N; pl.K = K; pl.prec = prec;
+  pl.kmax = pick_kmax(K);
+  int W = 0, CH = 0;
+#define CFG64(KM) cfg_of<double, KM>(W, CH)
+#define CFG32(KM) cfg_of<float, KM>(W, CH)
+  if (prec == ADX_F64) { ADX_KMAX_SWITCH(pl.kmax, CFG64) } else { ADX_KMAX_SWITCH(pl.kmax, CFG32) }
+#undef CFG64
+#undef CFG32
+  pl.W = W; pl.CH = CH;
+  pl.elem_size = prec == ADX_F64 ? sizeof(double) : sizeof(float);
+  pl.n_stile = ceil_div(N, W);
+  // minimise split*2MK + mblk*NK with split*mblk ~ PLAN_BLOCKS
+  double s = sqrt((double)PLAN_BLOCKS * (double)N / (2.0 * (double)M));
+  int64_t n_split = (int64_t)llround(s);
+  n_split = n_split < 1 ? 1 : n_split;
+  n_split = n_split > pl.n_stile ? pl.n_stile : n_split;
+  int64_t max_mblk = ceil_div(M, CH);
+  int64_t n_mblk = ceil_div(PLAN_BLOCKS, n_split);
+  n_mblk = n_mblk < 1 ? 1 : (n_mblk > max_mblk ? max_mblk : n_mblk);
+  int64_t mb = ceil_div(ceil_div(M, n_mblk), CH) * CH;
+  n_mblk = ceil_div(M, mb);
+  pl.n_split = (int)n_split;
+  pl.n_mblk = (int)n_mblk;
+  pl.mb = mb;
+  pl.ab_elems = (size_t)n_split * (size_t)M * 2 * K;
+  pl.t_elems = (size_t)n_mblk * (size_t)N * K;
+  return ADX_OK;
+}
+
+template <typename R>
+static int launch_sweep(const EmPlan& pl, const uint8_t* G, const void* P, const void* Q, void* ws,
+                        cudaStream_t st) {
+  R* ABp = reinterpret_cast<R*>(ws);
+  R* Tp = ABp + pl.ab_elems;
+  const dim3 grid((unsigned)(pl.n_split * pl.n_mblk));
+#define LAUNCH(KM)                                                                              \
+  em_sweep_kernel<R, KM><<<grid, TPB, 0, st>>>(G, (const R*)P, (const R*)Q, pl.M, pl.N, pl.K,   \
+                                               pl.n_stile, pl.n_split, pl.n_mblk, pl.mb, ABp, Tp)
+  ADX_KMAX_SWITCH(pl.kmax, LAUNCH)
+#undef LAUNCH
+  ADX_LAUNCH_CHECK();
+  return ADX_OK;
+}
+
+template <typename R>
+static int launch_update(const EmPlan& pl, void* ws, int mode, double* A, double* B, double* T,
+                         const double* q_bat, double* P, double* Q, float* P32, float* Q32,
+                         double* mP, double* vP, double* mQ, double* vQ, AdamArgs ad,
+                         cudaStream_t st) {
+  const R* ABp = reinterpret_cast<const R*>(ws);
+  const R* Tp = ABp + pl.ab_elems;
+  const int threads = 128;
+  const dim3 grid((unsigned)ceil_div(pl.M + pl.N, threads));
+#define LAUNCH(KM)                                                                          \
+  em_update_kernel<R, KM><<<grid, threads, 0, st>>>(ABp, Tp, pl.M, pl.N, pl.K, pl.n_split,  \
+                                                    pl.n_mblk, mode, A, B, T, q_bat, P, Q,  \
+                                                    P32, Q32, mP, vP, mQ, vQ, ad)
+  ADX_KMAX_SWITCH(pl.kmax, LAUNCH)
+#undef LAUNCH
+  ADX_LAUNCH_CHECK();
+  return ADX_OK;
+}
+
+int em_sweep(const EmPlan& pl, const uint8_t* G, const void* P, const void* Q, void* ws,
+             cudaStream_t st) {
+  return pl.prec == ADX_F64 ? launch_sweep<double>(pl, G, P, Q, ws, st)
+                            : launch_sweep<float>(pl, G, P, Q, ws, st);
+}
+
+int em_update(const EmPlan& pl, void* ws, int mode, double* A, double* B, double* T,
+              const double* q_bat, double* P, double* Q, float* P32, float* Q32, double* mP,
+              double* vP, double* mQ, double* vQ, AdamArgs ad, cudaStream_t st) {
+  return pl.prec == ADX_F64
+             ? launch_update<double>(pl, ws, mode, A, B, T, q_bat, P, Q, P32, Q32, mP, vP, mQ, vQ, ad, st)
+             : launch_update<float>(pl, ws, mode, A, B, T, q_bat, P, Q, P32, Q32, mP, vP, mQ, vQ, ad, st);
+}
+
+// Elementwise kernels for the unfused API (em_final_update and step as separate calls).
+__global__ void em_targets_kernel(const double* __restrict__ P, const double* __restrict__ Q,
+                                  const double* __restrict__ A, const double* __restrict__ B,
+                                  const double* __restrict__ T, const double* __restrict__ q_bat,
+                                  int64_t M, int64_t N, int K, double* __restrict__ P_EM,
+                                  double* __restrict__ Q_EM) {
+  const int64_t row = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (row < M) {
+    for (int k = 0; k < K; ++k) {
+      const int64_t o = row * K + k;
+      const double den = fmax((A[o] - B[o]) * P[o] + B[o], 1e-5);
+      P_EM[o] = ((1.0 / den) * P[o]) * A[o];
+    }
+  } else if (row < M + N) {
+    const int64_t i = row - M;
+    const double scale = 1.0 / fmax(q_bat[i], 1e-5);
+    double s = 0.0;
+    for (int k = 0; k < K; ++k) s += (Q[i * K + k] * T[i * K + k]) * scale;
+    s = fmax(s, 1e-5);
+    for (int k = 0; k < K; ++k) Q_EM[i * K + k] = ((Q[i * K + k] * T[i * K + k]) * scale) / s;
+  }
+}
+
+__global__ void adam_step_kernel(double* __restrict__ P, double* __restrict__ Q,
+                                 const double* __restrict__ P_EM, const double* __restrict__ Q_EM,
+                                 double* __restrict__ mP, double* __restrict__ vP,
+                                 double* __restrict__ mQ, double* __restrict__ vQ, int64_t M,
+                                 int64_t N, int K, AdamArgs ad, float* __restrict__ P32,
+                                 float* __restrict__ Q32) {
+  const int64_t row = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (row >= M + N) return;
+  const double bc1 = 1.0 - pow(ad.b1, ad.t);
+  const double bc2 = 1.0 - pow(ad.b2, ad.t);
+  const bool isP = row < M;
+  const int64_t r = isP ? row : row - M;
+  double* X = isP ? P : Q;
+  const double* Xt = isP ? P_EM : Q_EM;
+  double* m = isP ? mP : mQ;
+  double* v = isP ? vP : vQ;
+  float* X32 = isP ? P32 : Q32;
+  double tot = 0.0;
+  for (int k = 0; k < K; ++k) {
+    const int64_t o = r * K + k;
+    const double x = X[o];
+    const double delta = Xt[o] - x;
+    const double mm = m[o] * ad.b1 + (1.0 - ad.b1) * delta;
+    const double vv = v[o] * ad.b2 + (1.0 - ad.b2) * (delta * delta);
+    m[o] = mm;
+    v[o] = vv;
+    double nx = x + (ad.lr * (mm / bc1)) / (sqrt(vv / bc2) + ad.eps);
+    nx = fmin(fmax(nx, DOMAIN), 1.0 - DOMAIN);
+    X[o] = nx;
+    tot += nx;
+  }
+  for (int k = 0; k < K; ++k) {
+    const int64_t o = r * K + k;
+    if (!isP) X[o] = X[o] / tot;
+    if (X32) X32[o] = (float)X[o];
+  }
+}
+
+}  // namespace adx
+
+using namespace adx;
+
+extern "C" int adx_em_workspace_bytes(int64_t M, int64_t N, int K, int precision, size_t* bytes) {
+  if (!bytes) return ADX_ERR_ARG;
+  EmPlan pl;
+  const int rc = em_plan(M, N, K, precision, pl);
+  if (rc) { adx_set_message("adx_em_workspace_bytes: bad shape or precision"); return rc; }
+  *bytes = pl.bytes();
+  return ADX_OK;
+}
+
+extern "C" int adx_em_stats(const uint8_t* G, int64_t M, int64_t N, int K, int precision,
+                            const void* P, const void* Q, double* A, double* B, double* T,
+                            void* workspace, size_t workspace_bytes, void* stream) {
+  EmPlan pl;
+  int rc = em_plan(M, N, K, precision, pl);
+  if (rc) { adx_set_message("adx_em_stats: bad shape or precision"); return rc; }
+  if (!G || !P || !Q || !A || !B || !T || !workspace) { adx_set_message("adx_em_stats: null pointer"); return ADX_ERR_ARG; }
+  if (workspace_bytes < pl.bytes()) { adx_set_message("adx_em_stats: workspace too small"); return ADX_ERR_WORKSPACE; }
+  cudaStream_t st = as_stream(stream);
+  rc = em_sweep(pl, G, P, Q, workspace, st);
+  if (rc) return rc;
+  return em_update(pl, workspace, 0, A, B, T, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr,
+                   nullptr, nullptr, nullptr, AdamArgs{1, 0, 0, 0, 0}, st);
+}
+
+extern "C" int adx_em_sweep(const uint8_t* G, int64_t M, int64_t N, int K, int precision,
+                            const void* P, const void* Q, void* workspace, size_t workspace_bytes,
+                            void* stream) {
+  EmPlan pl;
+  int rc = em_plan(M, N, K, precision, pl);
+  if (rc) { adx_set_message("adx_em_sweep: bad shape or precision"); return rc; }
+  if (!G || !P || !Q || !workspace) { adx_set_message("adx_em_sweep: null pointer"); return ADX_ERR_ARG; }
+  if (workspace_bytes < pl.bytes()) { adx_set_message("adx_em_sweep: workspace too small"); return ADX_ERR_WORKSPACE; }
+  return em_sweep(pl, G, P, Q, workspace, as_stream(stream));
+}
+
+extern "C" int adx_em_targets(const double* P, const double* Q, const double* A, const double* B,
+                              const double* T, const double* q_bat, int64_t M, int64_t N, int K,
+                              double* P_EM, double* Q_EM, void* stream) {
+  if (M <= 0 || N <= 0 || K < 1 || K > ADX_MAX_K) { adx_set_message("adx_em_targets: bad shape"); return ADX_ERR_ARG; }
+  const int threads = 128;
+  em_targets_kernel<<<(unsigned)ceil_div(M + N, threads), threads, 0, as_stream(stream)>>>(
+      P, Q, A, B, T, q_bat, M, N, K, P_EM, Q_EM);
+  ADX_LAUNCH_CHECK();
+  return ADX_OK;
+}
+
+extern "C" int adx_adam_step(double* P, double* Q, const double* P_EM, const double* Q_EM,
+                             double* mP, double* vP, double* mQ, double* vQ, int64_t M, int64_t N,
+                             int K, double t, double lr, double beta1, double beta2, double eps,
+                             float* P32, float* Q32, void* stream) {
+  if (M <= 0 || N <= 0 || K < 1 || K > ADX_MAX_K || t < 1) { adx_set_message("adx_adam_step: bad arguments"); return ADX_ERR_ARG; }
+  const int threads = 128;
+  adam_step_kernel<<<(unsigned)ceil_div(M + N, threads), threads, 0, as_stream(stream)>>>(
+      P, Q, P_EM, Q_EM, mP, vP, mQ, vQ, M, N, K, AdamArgs{t, lr, beta1, beta2, eps}, P32, Q32);
+  ADX_LAUNCH_CHECK();
+  return ADX_OK;
+}
+
+extern "C" int adx_em_adam_iteration(const uint8_t* G, int64_t M, int64_t N, int K, int precision,
+                                     double* P, double* Q, float* P32, float* Q32, double* mP,
+                                     double* vP, double* mQ, double* vQ, const double* q_bat,
+                                     double t, double lr, double beta1, double beta2, double eps,
+                                     void* workspace, size_t workspace_bytes, void* stream) {
+  EmPlan pl;
+  int rc = em_plan(M, N, K, precision, pl);
+  if (rc) { adx_set_message("adx_em_adam_iteration: bad shape or precision"); return rc; }
+  if (!G || !P || !Q || !mP || !vP || !mQ || !vQ || !q_bat || !workspace || t < 1) {
+    adx_set_message("adx_em_adam_iteration: bad arguments");
+    return ADX_ERR_ARG;
+  }
+  if (precision != ADX_F64 && (!P32 || !Q32)) { adx_set_message("adx_em_adam_iteration: P32/Q32 required"); return ADX_ERR_ARG; }
+  if (workspace_bytes < pl.bytes()) { adx_set_message("adx_em_adam_iteration: workspace too small"); return ADX_ERR_WORKSPACE; }
+  cudaStream_t st = as_stream(stream);
+  const void* Pin = precision == ADX_F64 ? (const void*)P : (const void*)P32;
+  const void* Qin = precision == ADX_F64 ? (const void*)Q : (const void*)Q32;
+  rc = em_sweep(pl, G, Pin, Qin, workspace, st);
+  if (rc) return rc;
+  return em_update(pl, workspace, 1, nullptr, nullptr, nullptr, q_bat, P, Q, P32, Q32, mP, vP, mQ,
+                   vQ, AdamArgs{t, lr, beta1, beta2, eps}, st);
+}

@@ -1,0 +1,204 @@
+// Binomial log-likelihood of (P, Q) over the packed genotypes, float64 sum
+// (adamixture/model/em_adam_gpu.py:226-279):
+//   L = sum over observed (j,i) of g log h + (2-g) log(1-h),  h = clamp(P_j.Q_i, 1e-10, 1-1e-10).
+//
+// Instead of two float64 logarithms per entry, each thread multiplies the per-entry factor
+//   f = h^g (1-h)^(2-g)  (1 when missing)
+// into a float64 running product per sample slot and moves the binary exponent into an
+// integer every packed quad (4 entries: f >= 1e-20, so the product never leaves the normal
+// range). log(prod) + e*ln2 once per thread gives the same sum as the per-entry logs to
+// float64 rounding (each multiply adds <= 2^-53 relative error, i.e. <= 1.1e-16 absolute in
+// the log). h is formed in float64 (ADX_F64) or float32 (ADX_F32) from P and Q of that type.
+// Per-block float64 partials are summed by a one-block kernel in block order: deterministic.
+#include "common.cuh"
+
+#include <math.h>
+
+namespace adx {
+
+constexpr int LL_TPB = 256;
+constexpr int LL_BLOCKS = 1184;  // 8 per SM on 148 SMs; fixed so the summation order is
+
+template <typename R, int KMAX>
+struct LlCfg {
+  static constexpr int SPT = (sizeof(R) == 4) ? (KMAX <= 16 ? 4 : (KMAX <= 32 ? 2 : 1))
+                                              : (KMAX <= 16 ? 2 : 1);
+  static constexpr int CH = 32;
+};
+
+// Split x = m * 2^e with m in [0.5, 1): returns m, adds e to *e.
+__device__ __forceinline__ double renorm(double x, int& e) {
+  int hi = __double2hiint(x);
+  const int lo = __double2loint(x);
+  const int ex = ((hi >> 20) & 0x7FF) - 1022;
+  e += ex;
+  hi = (hi & 0x800FFFFF) | (1022 << 20);
+  return __hiloint2double(hi, lo);
+}
+
+template <typename R, int KMAX>
+__global__ void __launch_bounds__(LL_TPB)
+loglik_kernel(const uint8_t* __restrict__ G, const R* __restrict__ P, const R* __restrict__ Q,
+              int64_t M, int64_t N, int K, int64_t n_stile, int n_split, int n_mblk, int64_t mb,
+              double* __restrict__ partial) {
+  using C = LlCfg<R, KMAX>;
+  constexpr int SPT = C::SPT, CH = C::CH;
+  __shared__ R Ps[CH][KMAX];
+  __shared__ double wsum[LL_TPB / 32];
+  const int mblk = blockIdx.x % n_mblk;
+  const int split = blockIdx.x / n_mblk;
+  const int64_t j0 = (int64_t)mblk * mb;
+  const int64_t j1 = min(M, j0 + mb);
+  const int64_t W = (int64_t)LL_TPB * SPT;
+  double acc = 0.0;
+  for (int64_t st = split; st < n_stile; st += n_split) {
+    const int64_t i0 = st * W + (int64_t)threadIdx.x * SPT;
+    R q[SPT][KMAX];
+    double prod[SPT];
+    int ex[SPT];
+#pragma unroll
+    for (int u = 0; u < SPT; ++u) {
+      prod[u] = 1.0;
+      ex[u] = 0;
+#pragma unroll
+      for (int k = 0; k < KMAX; ++k) q[u][k] = (i0 + u < N && k < K) ? Q[(i0 + u) * K + k] : (R)0;
+    }
+    for (int64_t c0 = j0; c0 < j1; c0 += CH) {
+      const int cn = (int)min((int64_t)CH, j1 - c0);
+      __syncthreads();
+      for (int e = threadIdx.x; e < CH * KMAX; e += LL_TPB) {
+        const int jl = e / KMAX, k = e % KMAX;
+        Ps[jl][k] = (jl < cn && k < K) ? P[(c0 + jl) * K + k] : (R)0;
+      }
+      __syncthreads();
+      for (int qd = 0; qd < cn; qd += 4) {
+        const int64_t row = (c0 + qd) >> 2;
+        uint32_t bytes[SPT];
+#pragma unroll
+        for (int u = 0; u < SPT; ++u) bytes[u] = (i0 + u < N) ? (uint32_t)__ldg(G + row * N + i0 + u) : 0xFFu;
+#pragma unroll
+        for (int s = 0; s < 4; ++s) {
+          const int jl = qd + s;
+          if (jl >= cn) break;
+#pragma unroll
+          for (int u = 0; u < SPT; ++u) {
+            const unsigned g = genotype(bytes[u], s);
+            R h = 0;
+#pragma unroll
+            for (int k = 0; k < KMAX; ++k) h += Ps[jl][k] * q[u][k];
+            const double hd = fmin(fmax((double)h, LL_CLAMP), 1.0 - LL_CLAMP);
+            const double om = 1.0 - hd;
+            const double f = g == 0u ? om * om : (g == 1u ? hd * om : (g == 2u ? hd * hd : 1.0));
+            prod[u] *= f;
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < SPT; ++u) prod[u] = renorm(prod[u], ex[u]);
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < SPT; ++u) acc += log(prod[u]) + (double)ex[u] * 0.69314718055994530942;
+  }
+  // block reduction in fixed order
+#pragma unroll
+  for (int o = 16; o >= 1; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  if ((threadIdx.x & 31) == 0) wsum[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s = 0.0;
+    for (int w = 0; w < LL_TPB / 32; ++w) s += wsum[w];
+    partial[blockIdx.x] = s;
+  }
+}
+
+__global__ void sum_partials_kernel(const double* __restrict__ partial, int n, double* __restrict__ out) {
+  __shared__ double sh[256];
+  double s = 0.0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) s += partial[i];
+  sh[threadIdx.x] = s;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w >= 1; w >>= 1) {
+    if ((int)threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) *out = sh[0];
+}
+
+int pick_kmax(int K);
+
+struct LlPlan {
+  int kmax, spt;
+  int64_t n_stile;
+  int n_split, n_mblk;
+  int64_t mb;
+};
+
+template <typename R, int KMAX>
+static int spt_of() { return LlCfg<R, KMAX>::SPT; }
+
+#define ADX_LL_KMAX_SWITCH(kmax, MACRO)                                                \
+  switch (kmax) {                                                                      \
+    case 2: MACRO(2); break;   case 3: MACRO(3); break;   case 4: MACRO(4); break;     \
+    case 6: MACRO(6); break;   case 8: MACRO(8); break;   case 10: MACRO(10); break;   \
+    case 12: MACRO(12); break; case 16: MACRO(16); break; case 24: MACRO(24); break;   \
+    case 32: MACRO(32); break; case 48: MACRO(48); break; case 64: MACRO(64); break;   \
+    default: break;                                                                    \
+  }
+
+static int ll_plan(int64_t M, int64_t N, int K, int prec, LlPlan& pl) {
+  if (M <= 0 || N <= 0 || K < 1 || K > ADX_MAX_K) return ADX_ERR_ARG;
+  if (prec != ADX_F64 && prec != ADX_F32 && prec != ADX_BF16) return ADX_ERR_UNSUPPORTED;
+  pl.kmax = pick_kmax(K);
+  int spt = 1;
+#define S64(KM) spt = spt_of<double, KM>()
+#define S32(KM) spt = spt_of<float, KM>()
+  if (prec == ADX_F64) { ADX_LL_KMAX_SWITCH(pl.kmax, S64) } else { ADX_LL_KMAX_SWITCH(pl.kmax, S32) }
+#undef S64
+#undef S32
+  pl.spt = spt;
+  pl.n_stile = ceil_div(N, (int64_t)LL_TPB * spt);
+  int64_t n_split = pl.n_stile < 8 ? pl.n_stile : 8;
+  int64_t n_mblk = ceil_div(LL_BLOCKS, n_split);
+  const int64_t max_mblk = ceil_div(M, 32);
+  n_mblk = n_mblk > max_mblk ? max_mblk : n_mblk;
+  int64_t mb = ceil_div(ceil_div(M, n_mblk), 32) * 32;
+  n_mblk = ceil_div(M, mb);
+  pl.n_split = (int)n_split;
+  pl.n_mblk = (int)n_mblk;
+  pl.mb = mb;
+  return ADX_OK;
+}
+
+}  // namespace adx
+
+using namespace adx;
+
+extern "C" int adx_loglik_workspace_bytes(int64_t M, int64_t N, int K, int precision, size_t* bytes) {
+  LlPlan pl;
+  const int rc = ll_plan(M, N, K, precision, pl);
+  if (rc || !bytes) { adx_set_message("adx_loglik_workspace_bytes: bad arguments"); return rc ? rc : ADX_ERR_ARG; }
+  *bytes = (size_t)pl.n_split * pl.n_mblk * sizeof(double) + 256;
+  return ADX_OK;
+}
+
+extern "C" int adx_loglik(const uint8_t* G, int64_t M, int64_t N, int K, int precision,
+                          const void* P, const void* Q, double* out, void* workspace,
+                          size_t workspace_bytes, void* stream) {
+  LlPlan pl;
+  int rc = ll_plan(M, N, K, precision, pl);
+  if (rc) { adx_set_message("adx_loglik: bad shape or precision"); return rc; }
+  if (!G || !P || !Q || !out || !workspace) { adx_set_message("adx_loglik: null pointer"); return ADX_ERR_ARG; }
+  const int nblk = pl.n_split * pl.n_mblk;
+  if (workspace_bytes < (size_t)nblk * sizeof(double)) { adx_set_message("adx_loglik: workspace too small"); return ADX_ERR_WORKSPACE; }
+  double* part = reinterpret_cast<double*>(workspace);
+  cudaStream_t st = as_stream(stream);
+#define L64(KM) loglik_kernel<double, KM><<<nblk, LL_TPB, 0, st>>>(G, (const double*)P, (const double*)Q, M, N, K, pl.n_stile, pl.n_split, pl.n_mblk, pl.mb, part)
+#define L32(KM) loglik_kernel<float, KM><<<nblk, LL_TPB, 0, st>>>(G, (const float*)P, (const float*)Q, M, N, K, pl.n_stile, pl.n_split, pl.n_mblk, pl.mb, part)
+  if (precision == ADX_F64) { ADX_LL_KMAX_SWITCH(pl.kmax, L64) } else { ADX_LL_KMAX_SWITCH(pl.kmax, L32) }
+#undef L64
+#undef L32
+  ADX_LAUNCH_CHECK();
+  sum_partials_kernel<<<1, 256, 0, st>>>(part, nblk, out);
+  ADX_LAUNCH_CHECK();
+  return ADX_OK;
+}

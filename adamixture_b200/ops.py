@@ -1,0 +1,266 @@
+"""Torch-facing wrappers of the CUDA library (device tensors in, device tensors out).
+
+Every function launches on the current torch CUDA stream of the tensors' device and
+raises on any error; nothing here runs on the CPU. Operator names registered with
+``register_reference_ops()`` match the reference's ``TORCH_LIBRARY`` schemas
+(adamixture/src/utils_c/cuda/pack2bit.cu:147-160) so its Python resolves to these kernels.
+"""
+from __future__ import annotations
+
+import torch
+
+from . import _lib
+from ._lib import ADX_BF16, ADX_F32, ADX_F64, call, query_size
+
+PRECISIONS = {"f64": ADX_F64, "f32": ADX_F32, "bf16": ADX_BF16}
+_TORCH_OF = {ADX_F64: torch.float64, ADX_F32: torch.float32, ADX_BF16: torch.float32}
+
+
+def precision_code(p) -> int:
+    if isinstance(p, int):
+        return p
+    try:
+        return PRECISIONS[p]
+    except KeyError:
+        raise ValueError(f"unknown precision {p!r}; use one of {sorted(PRECISIONS)}") from None
+
+
+def input_dtype(precision) -> torch.dtype:
+    """dtype of the P/Q operands an E-step of this precision reads."""
+    return _TORCH_OF[precision_code(precision)]
+
+
+def _ptr(t: torch.Tensor | None) -> int | None:
+    return None if t is None else t.data_ptr()
+
+
+def _stream(dev: torch.device) -> int:
+    return torch.cuda.current_stream(dev).cuda_stream
+
+
+def _check(t: torch.Tensor, name: str, dtype=None, device=None) -> None:
+    if not t.is_cuda:
+        raise ValueError(f"{name} must be a CUDA tensor (got {t.device})")
+    if not t.is_contiguous():
+        raise ValueError(f"{name} must be contiguous")
+    if dtype is not None and t.dtype != dtype:
+        raise ValueError(f"{name} must be {dtype} (got {t.dtype})")
+    if device is not None and t.device != device:
+        raise ValueError(f"{name} is on {t.device}, expected {device}")
+
+
+class Workspace:
+    """Grow-only device scratch buffer per device (caller-owned memory for the C ABI)."""
+
+    _bufs: dict = {}
+
+    @classmethod
+    def get(cls, device: torch.device, nbytes: int) -> torch.Tensor:
+        key = (device.type, device.index)
+        buf = cls._bufs.get(key)
+        if buf is None or buf.numel() < nbytes:
+            cls._bufs[key] = None
+            buf = torch.empty(max(nbytes, 256), dtype=torch.uint8, device=device)
+            cls._bufs[key] = buf
+        return buf
+
+    @classmethod
+    def release(cls) -> None:
+        cls._bufs.clear()
+
+
+# ---------------------------------------------------------------- genotype layout
+
+def unpack_u8(G: torch.Tensor, m_start: int, count: int, M: int, byte_offset: int = 0) -> torch.Tensor:
+    """Decode SNP rows [m_start, m_start+count) of packed ``G`` to ``[count, N]`` uint8."""
+    _check(G, "G", torch.uint8)
+    N = G.shape[1]
+    count = max(0, min(count, M - m_start))
+    out = torch.empty((count, N), dtype=torch.uint8, device=G.device)
+    if count:
+        call("adx_unpack_u8", G.data_ptr(), G.shape[0], N, M, m_start, count, byte_offset,
+             out.data_ptr(), _stream(G.device))
+    return out
+
+
+def unpack_center(G: torch.Tensor, f: torch.Tensor, m_start: int, count: int, M: int,
+                  byte_offset: int = 0) -> torch.Tensor:
+    """Decode and centre: ``g - 2 f_j`` (0 where missing), float32 ``[count, N]``."""
+    _check(G, "G", torch.uint8)
+    _check(f, "f", torch.float32, G.device)
+    N = G.shape[1]
+    count = max(0, min(count, M - m_start))
+    out = torch.empty((count, N), dtype=torch.float32, device=G.device)
+    if count:
+        call("adx_unpack_center_f32", G.data_ptr(), G.shape[0], N, M, m_start, count,
+             byte_offset, f.data_ptr(), out.data_ptr(), _stream(G.device))
+    return out
+
+
+def allele_frequency(G: torch.Tensor, M: int) -> torch.Tensor:
+    _check(G, "G", torch.uint8)
+    f = torch.empty(M, dtype=torch.float32, device=G.device)
+    call("adx_allele_frequency", G.data_ptr(), M, G.shape[1], f.data_ptr(), _stream(G.device))
+    return f
+
+
+def sample_counts(G: torch.Tensor, M: int) -> torch.Tensor:
+    """q_bat: 2 x observed SNPs per sample (float64)."""
+    _check(G, "G", torch.uint8)
+    q = torch.empty(G.shape[1], dtype=torch.float64, device=G.device)
+    call("adx_sample_counts", G.data_ptr(), M, G.shape[1], q.data_ptr(), _stream(G.device))
+    return q
+
+
+def bed_to_packed(bed_rows: torch.Tensor, N: int, M: int) -> torch.Tensor:
+    """PLINK BED rows ``[M, ceil(N/4)]`` (device) -> packed ``[ceil(M/4), N]``, flipped
+    0<->2 when the mean dosage/2 is >= 0.5 (the reference reader's rule)."""
+    _check(bed_rows, "bed_rows", torch.uint8)
+    dev = bed_rows.device
+    G = torch.empty(((M + 3) // 4, N), dtype=torch.uint8, device=dev)
+    nbytes = query_size("adx_bed_workspace_bytes", M, N)
+    ws = Workspace.get(dev, nbytes)
+    flipped = torch.zeros(1, dtype=torch.int32, device=dev)
+    call("adx_bed_to_packed", bed_rows.data_ptr(), M, N, G.data_ptr(), flipped.data_ptr(),
+         ws.data_ptr(), ws.numel(), _stream(dev))
+    return G
+
+
+def simulate_packed(Pq: torch.Tensor, Qq: torch.Tensor, miss_q: int, keys: tuple[int, int]) -> torch.Tensor:
+    """Sample packed genotypes on the device from fixed-point P/Q (see src/simulate.py)."""
+    _check(Pq, "Pq", torch.int32)
+    _check(Qq, "Qq", torch.int32, Pq.device)
+    M, K = Pq.shape
+    N = Qq.shape[0]
+    G = torch.empty(((M + 3) // 4, N), dtype=torch.uint8, device=Pq.device)
+    call("adx_simulate_packed", Pq.data_ptr(), Qq.data_ptr(), M, N, K, keys[0], keys[1],
+         miss_q, G.data_ptr(), _stream(Pq.device))
+    return G
+
+
+# ---------------------------------------------------------------- Adam-EM
+
+def em_workspace_bytes(M: int, N: int, K: int, precision) -> int:
+    return query_size("adx_em_workspace_bytes", M, N, K, precision_code(precision))
+
+
+def em_stats(G: torch.Tensor, P: torch.Tensor, Q: torch.Tensor, M: int, precision="f64"):
+    """Sufficient statistics (A, B, T) of one E-step sweep, float64."""
+    pc = precision_code(precision)
+    dt = input_dtype(pc)
+    _check(G, "G", torch.uint8)
+    _check(P, "P", dt, G.device)
+    _check(Q, "Q", dt, G.device)
+    N, K = Q.shape
+    dev = G.device
+    A = torch.empty((M, K), dtype=torch.float64, device=dev)
+    B = torch.empty((M, K), dtype=torch.float64, device=dev)
+    T = torch.empty((N, K), dtype=torch.float64, device=dev)
+    ws = Workspace.get(dev, em_workspace_bytes(M, N, K, pc))
+    call("adx_em_stats", G.data_ptr(), M, N, K, pc, P.data_ptr(), Q.data_ptr(), A.data_ptr(),
+         B.data_ptr(), T.data_ptr(), ws.data_ptr(), ws.numel(), _stream(dev))
+    return A, B, T
+
+
+def em_sweep(G: torch.Tensor, P: torch.Tensor, Q: torch.Tensor, M: int, precision,
+             workspace: torch.Tensor) -> None:
+    """The E-step sweep alone (partials left in ``workspace``)."""
+    pc = precision_code(precision)
+    N, K = Q.shape
+    call("adx_em_sweep", G.data_ptr(), M, N, K, pc, P.data_ptr(), Q.data_ptr(),
+         workspace.data_ptr(), workspace.numel(), _stream(G.device))
+
+
+def em_targets(P, Q, A, B, T, q_bat, P_EM=None, Q_EM=None):
+    M, K = P.shape
+    N = Q.shape[0]
+    for t, n in ((P, "P"), (Q, "Q"), (A, "A"), (B, "B"), (T, "T"), (q_bat, "q_bat")):
+        _check(t, n, torch.float64, P.device)
+    P_EM = torch.empty_like(P) if P_EM is None else P_EM
+    Q_EM = torch.empty_like(Q) if Q_EM is None else Q_EM
+    call("adx_em_targets", P.data_ptr(), Q.data_ptr(), A.data_ptr(), B.data_ptr(), T.data_ptr(),
+         q_bat.data_ptr(), M, N, K, P_EM.data_ptr(), Q_EM.data_ptr(), _stream(P.device))
+    return P_EM, Q_EM
+
+
+def adam_step(P, Q, P_EM, Q_EM, mP, vP, mQ, vQ, t, lr, beta1, beta2, eps, P32=None, Q32=None):
+    M, K = P.shape
+    N = Q.shape[0]
+    for x, n in ((P, "P"), (Q, "Q"), (P_EM, "P_EM"), (Q_EM, "Q_EM"), (mP, "m_P"), (vP, "v_P"),
+                 (mQ, "m_Q"), (vQ, "v_Q")):
+        _check(x, n, torch.float64, P.device)
+    call("adx_adam_step", P.data_ptr(), Q.data_ptr(), P_EM.data_ptr(), Q_EM.data_ptr(),
+         mP.data_ptr(), vP.data_ptr(), mQ.data_ptr(), vQ.data_ptr(), M, N, K, float(t),
+         float(lr), float(beta1), float(beta2), float(eps), _ptr(P32), _ptr(Q32), _stream(P.device))
+
+
+def em_adam_iteration(G, P, Q, P32, Q32, mP, vP, mQ, vQ, q_bat, M, t, lr, beta1, beta2, eps,
+                      precision="f32", workspace: torch.Tensor | None = None):
+    """One fused Adam-EM iteration (E-step sweep + targets + Adam move), in place."""
+    pc = precision_code(precision)
+    N, K = Q.shape
+    dev = G.device
+    ws = workspace if workspace is not None else Workspace.get(dev, em_workspace_bytes(M, N, K, pc))
+    call("adx_em_adam_iteration", G.data_ptr(), M, N, K, pc, P.data_ptr(), Q.data_ptr(),
+         _ptr(P32), _ptr(Q32), mP.data_ptr(), vP.data_ptr(), mQ.data_ptr(), vQ.data_ptr(),
+         q_bat.data_ptr(), float(t), float(lr), float(beta1), float(beta2), float(eps),
+         ws.data_ptr(), ws.numel(), _stream(dev))
+
+
+def loglik_device(G: torch.Tensor, P: torch.Tensor, Q: torch.Tensor, M: int, precision="f64",
+                  out: torch.Tensor | None = None) -> torch.Tensor:
+    """Log-likelihood as a device float64 scalar (no host sync)."""
+    pc = precision_code(precision)
+    dt = input_dtype(pc)
+    _check(G, "G", torch.uint8)
+    _check(P, "P", dt, G.device)
+    _check(Q, "Q", dt, G.device)
+    N, K = Q.shape
+    dev = G.device
+    out = torch.empty((), dtype=torch.float64, device=dev) if out is None else out
+    nbytes = query_size("adx_loglik_workspace_bytes", M, N, K, pc)
+    ws = _ll_ws(dev, nbytes)
+    call("adx_loglik", G.data_ptr(), M, N, K, pc, P.data_ptr(), Q.data_ptr(), out.data_ptr(),
+         ws.data_ptr(), ws.numel(), _stream(dev))
+    return out
+
+
+_LL_WS: dict = {}
+
+
+def _ll_ws(dev, nbytes):
+    key = (dev.type, dev.index)
+    buf = _LL_WS.get(key)
+    if buf is None or buf.numel() < nbytes:
+        buf = torch.empty(max(nbytes, 256), dtype=torch.uint8, device=dev)
+        _LL_WS[key] = buf
+    return buf
+
+
+# ---------------------------------------------------------------- reference operator names
+
+_registered = False
+
+
+def register_reference_ops() -> None:
+    """Register ``pack2bit::unpack2bit_gpu_chunk_uint8`` and ``pack2bit::unpack2bit_gpu_chunk_center``
+    (same schemas as the reference) on the CUDA dispatch key, backed by this library."""
+    global _registered
+    if _registered:
+        return
+    lib = torch.library.Library("pack2bit", "DEF")
+    lib.define("unpack2bit_gpu_chunk_uint8(Tensor input, int m_start, int chunk_size, int M_total, "
+               "int byte_offset, int threads_per_block) -> Tensor")
+    lib.define("unpack2bit_gpu_chunk_center(Tensor input, Tensor f, int m_start, int chunk_size, "
+               "int M_total, int byte_offset, int threads_per_block) -> Tensor")
+
+    def _u8(inp, m_start, chunk_size, M_total, byte_offset, threads_per_block):
+        return unpack_u8(inp.contiguous(), m_start, chunk_size, M_total, byte_offset)
+
+    def _center(inp, f, m_start, chunk_size, M_total, byte_offset, threads_per_block):
+        return unpack_center(inp.contiguous(), f.contiguous(), m_start, chunk_size, M_total, byte_offset)
+
+    lib.impl("unpack2bit_gpu_chunk_uint8", _u8, "CUDA")
+    lib.impl("unpack2bit_gpu_chunk_center", _center, "CUDA")
+    register_reference_ops._lib = lib  # keep the registration alive
+    _registered = True

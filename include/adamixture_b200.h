@@ -1,0 +1,139 @@
+/*
+ * adamixture_b200: C ABI of the B200 (sm_100a) kernels for the ADMIXTURE Adam-EM hot path.
+ *
+ * Conventions
+ *  - Every pointer argument except host scalars is DEVICE memory; sizes are element counts.
+ *  - `stream` is a cudaStream_t passed as void*; NULL means the legacy default stream.
+ *    Every launch goes on `stream`; no call synchronises the device.
+ *  - Every entry point returns ADX_OK (0) or an ADX_ERR_* code; adx_last_error() returns a
+ *    message for the last failure on the calling host thread.
+ *  - Packed genotypes: uint8 G[ceil(M/4)][N], byte (j>>2)*N + i holds SNP j of sample i in
+ *    bits 2*(j&3); 0/1/2 = allele count, 3 = missing; unused bits of the last row are 0.
+ *    (The reference's GPU layout, adamixture/src/utils_c/cython/snp_reader.pyx:76-120.)
+ *  - P is [M][K], Q is [N][K], row-major. "precision" selects the E-step arithmetic:
+ *    ADX_F64 (float64, the reference GPU path's precision), ADX_F32, ADX_BF16
+ *    (tensor-core form, K >= 8). P/Q passed to a pass are double for ADX_F64 and float
+ *    otherwise.
+ *  - Calls that need scratch memory take a caller-allocated `workspace` whose size
+ *    adx_*_workspace_bytes() reports; none of them allocates device memory.
+ */
+#ifndef ADAMIXTURE_B200_H
+#define ADAMIXTURE_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+  ADX_OK = 0,
+  ADX_ERR_ARG = 1,          /* invalid size, K or pointer */
+  ADX_ERR_CUDA = 2,         /* a CUDA runtime call or launch failed */
+  ADX_ERR_WORKSPACE = 3,    /* workspace smaller than adx_*_workspace_bytes() */
+  ADX_ERR_UNSUPPORTED = 4,  /* precision/K combination not built */
+};
+
+enum { ADX_F64 = 0, ADX_F32 = 1, ADX_BF16 = 2 };
+
+/* Largest K the kernels accept (the reference's GPU limit, adamixture/entry.py:299-303). */
+#define ADX_MAX_K 64
+
+const char* adx_version(void);
+const char* adx_last_error(void);
+
+/* ---------------------------------------------------------------- genotype layout */
+
+/* Decode SNP rows [m_start, m_start+count) into out[count][N] (uint8, 3 = missing).
+ * G holds packed rows starting at packed row `byte_offset` (a host-streamed slice) and
+ * has `rows` packed rows. Replaces torch.ops.pack2bit.unpack2bit_gpu_chunk_uint8
+ * (adamixture/src/utils_c/cuda/pack2bit.cu:15-44, 83-111, 147-160). */
+int adx_unpack_u8(const uint8_t* G, int64_t rows, int64_t N, int64_t M_total, int64_t m_start,
+                  int64_t count, int64_t byte_offset, uint8_t* out, void* stream);
+
+/* Same rows decoded and centred: out = g - 2 f_j, 0 where missing (float32).
+ * Replaces torch.ops.pack2bit.unpack2bit_gpu_chunk_center (pack2bit.cu:46-77, 114-141). */
+int adx_unpack_center_f32(const uint8_t* G, int64_t rows, int64_t N, int64_t M_total,
+                          int64_t m_start, int64_t count, int64_t byte_offset, const float* f,
+                          float* out, void* stream);
+
+/* f_j = sum_i g_ij / (2 * #observed_j), 0 when none observed (float32).
+ * Replaces calculate_frequencies_gpu (adamixture/src/utils.py:781-861). */
+int adx_allele_frequency(const uint8_t* G, int64_t M, int64_t N, float* f, void* stream);
+
+/* q_bat_i = 2 * #observed SNPs of sample i (float64): the per-sample count that the
+ * reference re-accumulates on every E-step (adamixture/model/em_adam_gpu.py:76, 196). */
+int adx_sample_counts(const uint8_t* G, int64_t M, int64_t N, double* q_bat, void* stream);
+
+/* PLINK BED rows bed[M][ceil(N/4)] (SNP-major, LUT [2,3,1,0]) -> packed G, then the
+ * reference's 0<->2 flip when the mean dosage/2 is >= 0.5. `flipped` (device int) receives
+ * 1 when the flip was applied. Replaces read_bed_packed + get_mean_packed + flip_packed
+ * (adamixture/src/utils_c/cython/snp_reader.pyx:76-120, 215-303;
+ *  adamixture/src/snp_reader.py:747-757). workspace: adx_bed_workspace_bytes(). */
+int adx_bed_workspace_bytes(int64_t M, int64_t N, size_t* bytes);
+int adx_bed_to_packed(const uint8_t* bed, int64_t M, int64_t N, uint8_t* G, int* flipped,
+                      void* workspace, size_t workspace_bytes, void* stream);
+
+/* Synthetic cohort sampler (no counterpart in the reference; used for benchmarks):
+ * g = [u1 < h_q] + [u2 < h_q] with h_q = sum_k Pq[j][k] Qq[i][k] (16-bit fixed point,
+ * rows of Qq sum to 2^16), u1|u2 = splitmix64((j*N+i)*0x9E3779B97F4A7C15 + key1),
+ * missing when low32(splitmix64((j*N+i)*0x9E3779B97F4A7C15 + key2)) < miss_q. */
+int adx_simulate_packed(const uint32_t* Pq, const uint32_t* Qq, int64_t M, int64_t N, int K,
+                        uint64_t key1, uint64_t key2, uint32_t miss_q, uint8_t* G, void* stream);
+
+/* ---------------------------------------------------------------- Adam-EM */
+
+/* Scratch needed by adx_em_stats / adx_em_adam_iteration for this shape. */
+int adx_em_workspace_bytes(int64_t M, int64_t N, int K, int precision, size_t* bytes);
+
+/* One fused E-step sweep over G: A, B [M][K] and T [N][K] (float64), the sufficient
+ * statistics EMAdamOptimizer.run_em_step accumulates (A_accum, B_accum, T_accum;
+ * adamixture/model/em_adam_gpu.py:46-78 em_batch_math, 166-197 run_em_step).
+ * P, Q are double for ADX_F64, float otherwise. */
+int adx_em_stats(const uint8_t* G, int64_t M, int64_t N, int K, int precision, const void* P,
+                 const void* Q, double* A, double* B, double* T, void* workspace,
+                 size_t workspace_bytes, void* stream);
+
+/* The E-step sweep alone: the same single pass over G as adx_em_stats, leaving the
+ * per-block partial sums in `workspace` (for callers that time or combine the sweep). */
+int adx_em_sweep(const uint8_t* G, int64_t M, int64_t N, int K, int precision, const void* P,
+                 const void* Q, void* workspace, size_t workspace_bytes, void* stream);
+
+/* EM targets from the statistics (em_final_update, em_adam_gpu.py:82-117):
+ * P_EM = A P / max(P(A-B)+B, 1e-5); Q_EM = Q T / max(q_bat, 1e-5), rows / max(sum, 1e-5). */
+int adx_em_targets(const double* P, const double* Q, const double* A, const double* B,
+                   const double* T, const double* q_bat, int64_t M, int64_t N, int K,
+                   double* P_EM, double* Q_EM, void* stream);
+
+/* One Adam move toward the targets, then clamp P, Q to [1e-5, 1-1e-5] and renormalise Q
+ * rows (EMAdamOptimizer.step + adam_update, em_adam_gpu.py:11-42, 201-224). `t` is the
+ * step count after the increment. P32/Q32 (may be NULL) receive float copies. */
+int adx_adam_step(double* P, double* Q, const double* P_EM, const double* Q_EM, double* mP,
+                  double* vP, double* mQ, double* vQ, int64_t M, int64_t N, int K, double t,
+                  double lr, double beta1, double beta2, double eps, float* P32, float* Q32,
+                  void* stream);
+
+/* One whole Adam-EM iteration (run_em_step + step) in two launches: the fused E-step
+ * sweep, then one kernel that reduces the statistics, forms the EM targets and applies
+ * the Adam move to every P and Q row. Inputs of the sweep are P32/Q32 (float) for
+ * ADX_F32/ADX_BF16 and P/Q (double) for ADX_F64; P32/Q32 are refreshed. */
+int adx_em_adam_iteration(const uint8_t* G, int64_t M, int64_t N, int K, int precision,
+                          double* P, double* Q, float* P32, float* Q32, double* mP, double* vP,
+                          double* mQ, double* vQ, const double* q_bat, double t, double lr,
+                          double beta1, double beta2, double eps, void* workspace,
+                          size_t workspace_bytes, void* stream);
+
+/* Binomial log-likelihood, float64 sum: sum over observed entries of
+ * g log h + (2-g) log(1-h), h = clamp(P Q^T, 1e-10, 1-1e-10) (loglikelihood_gpu,
+ * em_adam_gpu.py:226-279). *out is a device double. */
+int adx_loglik_workspace_bytes(int64_t M, int64_t N, int K, int precision, size_t* bytes);
+int adx_loglik(const uint8_t* G, int64_t M, int64_t N, int K, int precision, const void* P,
+               const void* Q, double* out, void* workspace, size_t workspace_bytes,
+               void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* ADAMIXTURE_B200_H */

@@ -1,0 +1,167 @@
+"""Regenerate the golden fixtures in tests/golden/ from the reference implementation.
+
+Run from the repository root, in a tree that has the reference sources and the
+compiled reference modules (``make -C oracle``):
+
+    python tests/golden/make_golden.py
+
+What it records (all from the reference's own code, imported from its source tree;
+its ``torch.compile`` wrappers run eagerly as float64 torch code on the CPU, with the
+CUDA unpack op replaced by a bit-shift unpacker of the same packed layout):
+
+* ``demo.npz``: the reference demo cohort (105 samples x 8451 SNPs): raw BED rows,
+  the reference reader's packed and unpacked output (checked here against the
+  reference's reader fixtures), allele frequencies, the reference's GPU ALS init
+  (``demo/outputs/gpu/adamem/demo_run.als.*``), one ``EMAdamOptimizer.run_em_step``
+  from that init (A, B, T, q_bat, P_EM, Q_EM), a 20-iteration Adam-EM trace
+  (float32 P/Q snapshots after the priming step and after iterations 1, 2, 3, 5, 10,
+  15, 20, and every iteration's log-likelihood), and the converged ``optimize_parameters_gpu`` result.
+* ``synth.npz``: a seeded synthetic cohort (N=301, M=2003, K=8, 2% missing) with the
+  same records (trace of 10 iterations).
+* ``edge.npz``: a tiny cohort (N=37, M=29, K=4) with an all-missing sample and an
+  all-missing SNP, with one E-step and the log-likelihood.
+"""
+from __future__ import annotations
+
+import os
+import sys
+from pathlib import Path
+
+os.environ.setdefault("TORCHDYNAMO_DISABLE", "1")
+ROOT = Path(__file__).resolve().parents[2]
+sys.path.insert(0, str(ROOT))
+
+import numpy as np  # noqa: E402
+import torch  # noqa: E402
+
+from oracle import refmods  # noqa: E402
+
+OUT = Path(__file__).resolve().parent
+torch.set_num_threads(os.cpu_count() or 1)
+
+
+def torch_unpacker(G, start, count, M):
+    j = torch.arange(start, start + count)
+    rows = G[j >> 2].to(torch.int32)
+    return ((rows >> ((j & 3) * 2).to(torch.int32)[:, None]) & 3).to(torch.uint8)
+
+
+def reference():
+    refmods.import_reference()
+    from adamixture.model import em_adam_gpu
+    from adamixture.src import utils
+
+    utils.get_unpacker = lambda device, tpb: torch_unpacker
+    em_adam_gpu.utils.get_unpacker = utils.get_unpacker
+    return em_adam_gpu, utils
+
+
+HP = dict(lr=0.005, beta1=0.80, beta2=0.88, reg_adam=1e-8, check=5, lr_decay=0.5,
+          min_lr=1e-4, patience=3, tol=0.1)
+
+
+def run_records(em, utils, Gp, M, N, K, P0, Q0, trace_iters, converge=True):
+    """E-step, trace and converged run from (P0, Q0) through the reference code."""
+    dev = torch.device("cpu")
+    G = torch.from_numpy(Gp)
+    P = torch.from_numpy(P0.copy())
+    Q = torch.from_numpy(Q0.copy())
+    rec = {}
+    opt = em.EMAdamOptimizer(P.shape, Q.shape, HP["lr"], HP["beta1"], HP["beta2"], HP["reg_adam"], dev)
+    P_EM, Q_EM = opt.run_em_step(G, P, Q, M, 8192, torch_unpacker)
+    rec.update(A=opt.A_accum.numpy().copy(), B=opt.B_accum.numpy().copy(),
+               T=opt.T_accum.numpy().copy(), q_bat=opt.q_bat.numpy().copy(),
+               P_EM=P_EM.numpy().copy(), Q_EM=Q_EM.numpy().copy())
+    rec["loglik0"] = np.float64(em.loglikelihood_gpu(G, P, Q, M, N, 8192, dev, 1))
+    # The reference loop (em_adam_gpu.py:318-337) step by step, recording snapshots.
+    opt = em.EMAdamOptimizer(P.shape, Q.shape, HP["lr"], HP["beta1"], HP["beta2"], HP["reg_adam"], dev)
+    opt.run_em_step(G, P, Q, M, 8192, torch_unpacker)
+    opt.step(P, Q, opt.P_EM, opt.Q_EM)
+    snapsP, snapsQ, lls = [P.numpy().copy()], [Q.numpy().copy()], []
+    for it in range(trace_iters):
+        opt.run_em_step(G, P, Q, M, 8192, torch_unpacker)
+        opt.step(P, Q, opt.P_EM, opt.Q_EM)
+        snapsP.append(P.numpy().copy())
+        snapsQ.append(Q.numpy().copy())
+        lls.append(em.loglikelihood_gpu(G, P, Q, M, N, 8192, dev, 1))
+    keep = [t for t in (0, 1, 2, 3, 5, 10, 15, 20) if t <= trace_iters]
+    rec["trace_iters"] = np.array(keep)
+    # float32 snapshots: the per-iteration parity bar is 1e-5 absolute
+    rec["trace_P"] = np.stack([snapsP[t] for t in keep]).astype(np.float32)
+    rec["trace_Q"] = np.stack([snapsQ[t] for t in keep]).astype(np.float32)
+    rec["trace_loglik"] = np.array(lls)
+    if converge:
+        Pc, Qc = em.optimize_parameters_gpu(
+            G, torch.from_numpy(P0.copy()), torch.from_numpy(Q0.copy()), HP["lr"], HP["beta1"],
+            HP["beta2"], HP["reg_adam"], 10000, HP["check"], K, M, N, HP["lr_decay"],
+            HP["min_lr"], HP["patience"], HP["tol"], dev, 8192, 1)
+        rec["conv_P"] = Pc.numpy().copy()
+        rec["conv_Q"] = Qc.numpy().copy()
+        rec["conv_loglik"] = np.float64(em.loglikelihood_gpu(G, Pc, Qc, M, N, 8192, dev, 1))
+    return rec
+
+
+def demo(em, utils):
+    tree = refmods.REFERENCE_TREE / "adamixture" / "demo"
+    bed = tree / "data" / "demo_data.bed"
+    Gp_t, N, M = utils.read_data(str(bed), packed=True, chunk_size=8192, verbose=False)
+    G_u, N2, M2 = utils.read_data(str(bed), packed=False, chunk_size=8192, verbose=False)
+    assert (N, M) == (N2, M2)
+    Gp = Gp_t.numpy()
+    exp_p = np.loadtxt(tree / "outputs" / "reader" / "demo_data.G.packed.expected").astype(np.uint8)
+    exp_u = np.loadtxt(tree / "outputs" / "reader" / "demo_data.G.expected").astype(np.uint8)
+    assert np.array_equal(exp_p, Gp), "reference reader disagrees with its packed fixture"
+    assert np.array_equal(exp_u, G_u), "reference reader disagrees with its unpacked fixture"
+    nb = (N + 3) // 4
+    bed_rows = np.fromfile(bed, dtype=np.uint8, offset=3).reshape(-1, nb)
+    f = utils.calculate_frequencies_cpu(G_u, M, N, 8192)
+    als = tree / "outputs" / "gpu" / "adamem"
+    P0 = np.loadtxt(als / "demo_run.als.P.expected")
+    Q0 = np.loadtxt(als / "demo_run.als.Q.expected")
+    K = P0.shape[1]
+    rec = run_records(em, utils, Gp, M, N, K, P0, Q0, trace_iters=20)
+    np.savez_compressed(OUT / "demo.npz", N=N, M=M, K=K, bed_rows=bed_rows, packed=Gp,
+                        unpacked=G_u, freq=f, P0=P0, Q0=Q0, **rec)
+    print("demo.npz", N, M, K, rec["conv_loglik"])
+
+
+def synth(em, utils):
+    from adamixture_b200.src.simulate import make_cohort
+
+    N, M, K = 301, 2003, 8
+    coh = make_cohort(N, M, K, F=0.05, alpha=0.3, miss=0.02, seed=7)
+    Gp = coh.packed()
+    rng = np.random.default_rng(11)
+    P0 = np.clip(coh.P + rng.normal(0, 0.05, coh.P.shape), 1e-5, 1 - 1e-5)
+    Q0 = np.clip(coh.Q + rng.uniform(0, 0.2, coh.Q.shape), 1e-5, 1 - 1e-5)
+    Q0 /= Q0.sum(1, keepdims=True)
+    rec = run_records(em, utils, Gp, M, N, K, P0, Q0, trace_iters=10)
+    np.savez_compressed(OUT / "synth.npz", N=N, M=M, K=K, packed=Gp, P0=P0, Q0=Q0,
+                        Pq=coh.Pq, Qq=coh.Qq, miss_q=coh.miss_q,
+                        keys=np.array(coh.keys, dtype=np.uint64), **rec)
+    print("synth.npz", rec["conv_loglik"])
+
+
+def edge(em, utils):
+    from adamixture_b200.src.packing import pack
+
+    N, M, K = 37, 29, 4
+    rng = np.random.default_rng(3)
+    G = rng.integers(0, 3, size=(M, N)).astype(np.uint8)
+    G[rng.random((M, N)) < 0.1] = 3
+    G[:, 5] = 3      # a sample with no observed SNP
+    G[11, :] = 3     # a SNP with no observed sample
+    Gp = pack(G)
+    P0 = np.clip(rng.random((M, K)), 1e-5, 1 - 1e-5)
+    Q0 = rng.random((N, K))
+    Q0 /= Q0.sum(1, keepdims=True)
+    rec = run_records(em, utils, Gp, M, N, K, P0, Q0, trace_iters=3, converge=False)
+    np.savez_compressed(OUT / "edge.npz", N=N, M=M, K=K, packed=Gp, unpacked=G, P0=P0, Q0=Q0, **rec)
+    print("edge.npz", rec["loglik0"])
+
+
+if __name__ == "__main__":
+    em, utils = reference()
+    edge(em, utils)
+    synth(em, utils)
+    demo(em, utils)

@@ -1,0 +1,280 @@
+"""GPU parity of the CUDA path against the reference (golden fixtures) and the CPU oracle.
+
+Bars (written per test):
+  * decode / layout / counts / sampler: bit-exact;
+  * E-step statistics, float64 mode: rtol 1e-10 against the reference's float64 torch path;
+  * per-iteration P/Q, float64 mode: 1e-5 max abs (observed ~1e-12);
+  * per-iteration P/Q, float32 mode: 1e-5 max abs on the 301-sample cohort; on the
+    105-sample demo cohort 99.9% of entries within 1e-5 and all within 2e-4 (Adam divides
+    each step by sqrt(v), which scales a float32 rounding of a near-zero EM delta by
+    lr/|delta|: the bound shrinks like 1/sqrt(N));
+  * log-likelihood: 1e-12 relative (float64 h), 1e-6 relative (float32 h);
+  * converged log-likelihood: 1e-6 relative of the reference's converged value.
+"""
+import numpy as np
+import pytest
+import torch
+
+from oracle import em_oracle as orc
+
+pytestmark = pytest.mark.gpu
+
+
+def dev_t(x, dtype=None):
+    t = torch.from_numpy(np.ascontiguousarray(x)).cuda()
+    return t if dtype is None else t.to(dtype)
+
+
+@pytest.fixture(scope="module")
+def ops(cuda):
+    from adamixture_b200 import ops as _ops
+
+    return _ops
+
+
+# ------------------------------------------------------------------ layout
+
+@pytest.mark.parametrize("name", ["demo", "edge", "synth"])
+def test_unpack_bit_exact(ops, name, request):
+    d = request.getfixturevalue(name)
+    M = int(d["M"])
+    G = dev_t(d["packed"])
+    full = ops.unpack_u8(G, 0, M, M).cpu().numpy()
+    assert np.array_equal(full, orc.unpack(d["packed"], M))
+    # chunked with host-streamed slices (byte_offset), odd chunk sizes
+    for start, count in ((0, 1), (3, 9), (5, 8192), (M - 3, 100)):
+        bs = start // 4
+        be = (min(M, start + count) + 3) // 4
+        part = ops.unpack_u8(G[bs:be].contiguous(), start, count, M, bs).cpu().numpy()
+        assert np.array_equal(part, orc.unpack(d["packed"], M, start, count))
+
+
+def test_unpack_center(ops, demo):
+    M = int(demo["M"])
+    G = dev_t(demo["packed"])
+    f = dev_t(demo["freq"])
+    out = ops.unpack_center(G, f, 17, 999, M).cpu().numpy()
+    g = orc.unpack(demo["packed"], M, 17, 999).astype(np.float32)
+    exp = np.where(g == 3, np.float32(0), g - np.float32(2) * demo["freq"][17:17 + 999, None])
+    np.testing.assert_array_equal(out, exp)
+
+
+def test_allele_frequency(ops, demo, edge):
+    for d in (demo, edge):
+        M = int(d["M"])
+        f = ops.allele_frequency(dev_t(d["packed"]), M).cpu().numpy()
+        np.testing.assert_array_equal(f, orc.allele_frequency(orc.unpack(d["packed"], M)))
+    np.testing.assert_allclose(ops.allele_frequency(dev_t(demo["packed"]), int(demo["M"])).cpu().numpy(),
+                               demo["freq"], rtol=1e-6)
+
+
+@pytest.mark.parametrize("name", ["demo", "edge", "synth"])
+def test_sample_counts(ops, name, request):
+    d = request.getfixturevalue(name)
+    M = int(d["M"])
+    q = ops.sample_counts(dev_t(d["packed"]), M).cpu().numpy()
+    np.testing.assert_array_equal(q, d["q_bat"])
+
+
+def test_bed_to_packed_matches_reference_reader(ops, demo):
+    N, M = int(demo["N"]), int(demo["M"])
+    G = ops.bed_to_packed(dev_t(demo["bed_rows"]), N, M).cpu().numpy()
+    assert np.array_equal(G, demo["packed"])
+
+
+def test_bed_flip_rule(ops):
+    from adamixture_b200.src import packing
+
+    rng = np.random.default_rng(5)
+    for N, M in ((7, 13), (64, 33)):
+        G = rng.choice([0, 1, 2, 3], size=(M, N), p=[0.05, 0.15, 0.7, 0.1]).astype(np.uint8)  # mean > .5
+        nb = (N + 3) // 4
+        codes = np.array([3, 2, 0, 1], dtype=np.uint8)[G]
+        pad = np.zeros((M, nb * 4), np.uint8)
+        pad[:, :N] = codes
+        pad = pad.reshape(M, nb, 4)
+        rows = pad[..., 0] | (pad[..., 1] << 2) | (pad[..., 2] << 4) | (pad[..., 3] << 6)
+        exp = orc.bed_to_packed(rows, N)
+        assert orc.packed_mean(exp, M) >= 0.5
+        exp = orc.flip_packed(exp, M)
+        got = ops.bed_to_packed(dev_t(rows), N, M).cpu().numpy()
+        assert np.array_equal(got, exp)
+        assert np.array_equal(packing.bed_rows_to_packed(rows, N), orc.bed_to_packed(rows, N))
+
+
+def test_simulator_matches_host_sampler(ops, synth):
+    Pq = dev_t(synth["Pq"].astype(np.int32))
+    Qq = dev_t(synth["Qq"].astype(np.int32))
+    keys = tuple(int(k) for k in synth["keys"])
+    G = ops.simulate_packed(Pq, Qq, int(synth["miss_q"]), keys).cpu().numpy()
+    assert np.array_equal(G, synth["packed"])
+
+
+# ------------------------------------------------------------------ E-step
+
+@pytest.mark.parametrize("name", ["demo", "edge", "synth"])
+def test_em_stats_f64_matches_reference(ops, name, request):
+    d = request.getfixturevalue(name)
+    M = int(d["M"])
+    A, B, T = ops.em_stats(dev_t(d["packed"]), dev_t(d["P0"]), dev_t(d["Q0"]), M, "f64")
+    np.testing.assert_allclose(A.cpu().numpy(), d["A"], rtol=1e-10, atol=1e-9)
+    np.testing.assert_allclose(B.cpu().numpy(), d["B"], rtol=1e-10, atol=1e-9)
+    np.testing.assert_allclose(T.cpu().numpy(), d["T"], rtol=1e-10, atol=1e-9)
+    q = ops.sample_counts(dev_t(d["packed"]), M)
+    P_EM, Q_EM = ops.em_targets(dev_t(d["P0"]), dev_t(d["Q0"]), A, B, T, q)
+    np.testing.assert_allclose(P_EM.cpu().numpy(), d["P_EM"], rtol=1e-10, atol=1e-12)
+    np.testing.assert_allclose(Q_EM.cpu().numpy(), d["Q_EM"], rtol=1e-10, atol=1e-12)
+
+
+@pytest.mark.parametrize("name", ["demo", "edge", "synth"])
+def test_em_stats_f32_close_to_reference(ops, name, request):
+    d = request.getfixturevalue(name)
+    M = int(d["M"])
+    A, B, T = ops.em_stats(dev_t(d["packed"]), dev_t(d["P0"], torch.float32),
+                           dev_t(d["Q0"], torch.float32), M, "f32")
+    for got, ref in ((A, d["A"]), (B, d["B"]), (T, d["T"])):
+        got = got.cpu().numpy()
+        scale = np.abs(ref).max()
+        assert np.abs(got - ref).max() <= 2e-5 * scale
+
+
+@pytest.mark.parametrize("K", [1, 2, 3, 5, 8, 10, 13, 17, 33, 64])
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+def test_em_stats_random_shapes_vs_oracle(ops, K, prec):
+    rng = np.random.default_rng(K)
+    N, M = 1001 + K, 523 + 7 * K
+    G = rng.integers(0, 4, size=(M, N)).astype(np.uint8)
+    P = np.clip(rng.random((M, K)), 1e-5, 1 - 1e-5)
+    Q = rng.random((N, K))
+    Q /= Q.sum(1, keepdims=True)
+    A0, B0, T0, _ = orc.em_stats(G, P, Q)
+    dt = torch.float64 if prec == "f64" else torch.float32
+    A, B, T = ops.em_stats(dev_t(orc.pack(G)), dev_t(P, dt), dev_t(Q, dt), M, prec)
+    tol = 1e-11 if prec == "f64" else 3e-5
+    for got, ref in ((A, A0), (B, B0), (T, T0)):
+        err = np.abs(got.cpu().numpy() - ref).max() / np.abs(ref).max()
+        assert err <= tol, err
+
+
+def test_em_stats_large_tile_counts(ops):
+    # several sample sub-tiles and splits, a ragged last SNP block and sample tile
+    rng = np.random.default_rng(1)
+    N, M, K = 5 * 1024 + 3, 4 * 4096 + 5, 4
+    coh_G = rng.integers(0, 4, size=(M, N)).astype(np.uint8)
+    P = np.clip(rng.random((M, K)), 1e-5, 1 - 1e-5)
+    Q = rng.dirichlet(np.ones(K), size=N)
+    A0, B0, T0, _ = orc.em_stats(coh_G, P, Q)
+    A, B, T = ops.em_stats(dev_t(orc.pack(coh_G)), dev_t(P), dev_t(Q), M, "f64")
+    np.testing.assert_allclose(A.cpu().numpy(), A0, rtol=1e-10)
+    np.testing.assert_allclose(B.cpu().numpy(), B0, rtol=1e-10)
+    np.testing.assert_allclose(T.cpu().numpy(), T0, rtol=1e-10)
+
+
+# ------------------------------------------------------------------ iterations
+
+def _trace(d, precision, n):
+    """Reference loop (priming + n iterations) through the fused CUDA iteration."""
+    from adamixture_b200.model.em_adam_gpu import EMAdamOptimizer
+
+    M = int(d["M"])
+    G = dev_t(d["packed"])
+    P = dev_t(d["P0"]).clone()
+    Q = dev_t(d["Q0"]).clone()
+    P32, Q32 = P.float(), Q.float()
+    opt = EMAdamOptimizer(P.shape, Q.shape, 0.005, 0.80, 0.88, 1e-8, G.device, precision)
+    snaps = []
+    for it in range(n + 1):
+        opt.fused_iteration(G, P, Q, P32, Q32, M)
+        snaps.append((P.cpu().numpy().copy(), Q.cpu().numpy().copy()))
+    return snaps
+
+
+@pytest.mark.parametrize("name", ["demo", "synth", "edge"])
+def test_per_iteration_f64_within_1e5(ops, name, request):
+    d = request.getfixturevalue(name)
+    n = int(d["trace_iters"].max())
+    snaps = _trace(d, "f64", n)
+    for s, t in enumerate(d["trace_iters"]):
+        assert np.abs(snaps[t][0] - d["trace_P"][s]).max() <= 1e-5
+        assert np.abs(snaps[t][1] - d["trace_Q"][s]).max() <= 1e-5
+
+
+def test_unfused_api_matches_fused(ops, synth):
+    from adamixture_b200.model.em_adam_gpu import EMAdamOptimizer
+
+    M = int(synth["M"])
+    G = dev_t(synth["packed"])
+    P = dev_t(synth["P0"]).clone()
+    Q = dev_t(synth["Q0"]).clone()
+    opt = EMAdamOptimizer(P.shape, Q.shape, 0.005, 0.80, 0.88, 1e-8, G.device, "f64")
+    for _ in range(3):
+        P_EM, Q_EM = opt.run_em_step(G, P, Q, M, 8192)
+        opt.step(P, Q, P_EM, Q_EM)
+    fused = _trace(synth, "f64", 2)[-1]
+    np.testing.assert_allclose(P.cpu().numpy(), fused[0], atol=1e-13)
+    np.testing.assert_allclose(Q.cpu().numpy(), fused[1], atol=1e-13)
+
+
+def test_per_iteration_f32_synth_within_1e5(ops, synth):
+    n = int(synth["trace_iters"].max())
+    snaps = _trace(synth, "f32", n)
+    for s, t in enumerate(synth["trace_iters"]):
+        assert np.abs(snaps[t][0] - synth["trace_P"][s]).max() <= 1e-5
+        assert np.abs(snaps[t][1] - synth["trace_Q"][s]).max() <= 1e-5
+
+
+def test_per_iteration_f32_demo(ops, demo):
+    n = int(demo["trace_iters"].max())
+    snaps = _trace(demo, "f32", n)
+    for s, t in enumerate(demo["trace_iters"]):
+        for k in (0, 1):
+            err = np.abs(snaps[t][k] - (demo["trace_P"], demo["trace_Q"])[k][s])
+            assert err.max() <= 2e-4
+            assert np.quantile(err, 0.999) <= 1e-5
+
+
+@pytest.mark.parametrize("name", ["demo", "synth", "edge"])
+def test_loglik(ops, name, request):
+    d = request.getfixturevalue(name)
+    M = int(d["M"])
+    G = dev_t(d["packed"])
+    ref = float(d["loglik0"])
+    l64 = float(ops.loglik_device(G, dev_t(d["P0"]), dev_t(d["Q0"]), M, "f64").item())
+    l32 = float(ops.loglik_device(G, dev_t(d["P0"], torch.float32), dev_t(d["Q0"], torch.float32), M, "f32").item())
+    assert abs(l64 - ref) <= 1e-12 * abs(ref)
+    assert abs(l32 - ref) <= 1e-6 * abs(ref)
+
+
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+@pytest.mark.parametrize("name", ["demo", "synth"])
+def test_converged_loglik_within_1e6(ops, name, prec, request):
+    from adamixture_b200.model.em_adam_gpu import loglikelihood_gpu, optimize_parameters_gpu
+
+    d = request.getfixturevalue(name)
+    M, N, K = int(d["M"]), int(d["N"]), int(d["K"])
+    G = dev_t(d["packed"])
+    P, Q = optimize_parameters_gpu(G, dev_t(d["P0"]), dev_t(d["Q0"]), 0.005, 0.80, 0.88, 1e-8,
+                                   10000, 5, K, M, N, 0.5, 1e-4, 3, 0.1, G.device, 8192, 512,
+                                   precision=prec)
+    L = loglikelihood_gpu(G, P, Q, M, N, 8192, G.device, 512)
+    ref = float(d["conv_loglik"])
+    assert abs(L - ref) <= 1e-6 * abs(ref), (L, ref)
+    Qn = Q.cpu().numpy()
+    np.testing.assert_allclose(Qn.sum(1), 1.0, atol=1e-12)
+    assert Qn.min() >= 1e-5 - 1e-12 and P.min().item() >= 1e-5 - 1e-15
+
+
+def test_cpu_tensors_rejected(ops, demo):
+    from adamixture_b200.model.em_adam_gpu import loglikelihood_gpu
+
+    with pytest.raises(ValueError, match="CUDA"):
+        loglikelihood_gpu(torch.from_numpy(demo["packed"]), torch.zeros(3, 2), torch.zeros(3, 2),
+                          3, 3, 8192, torch.device("cpu"), 1)
+
+
+def test_reference_op_names(ops, demo):
+    ops.register_reference_ops()
+    M = int(demo["M"])
+    G = dev_t(demo["packed"])
+    out = torch.ops.pack2bit.unpack2bit_gpu_chunk_uint8(G, 100, 8192, M, 0, 512)
+    assert np.array_equal(out.cpu().numpy(), orc.unpack(demo["packed"], M, 100, 8192))
