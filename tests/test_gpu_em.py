@@ -261,7 +261,10 @@ def test_converged_loglik_within_1e6(ops, name, prec, request):
     assert abs(L - ref) <= 1e-6 * abs(ref), (L, ref)
     Qn = Q.cpu().numpy()
     np.testing.assert_allclose(Qn.sum(1), 1.0, atol=1e-12)
-    assert Qn.min() >= 1e-5 - 1e-12 and P.min().item() >= 1e-5 - 1e-15
+    # the reference clamps to [1e-5, 1-1e-5] after the Adam move and then renormalises
+    # rows whose sum an Adam move does not preserve, so entries can end a little under
+    # 1e-5 (em_adam_gpu.py:222-224)
+    assert Qn.min() > 0.5e-5 and P.min().item() >= 1e-5 - 1e-15
 
 
 def test_cpu_tensors_rejected(ops, demo):
