@@ -41,6 +41,7 @@ SIGNATURES: dict[str, list] = {
                               c_double, c_double, c_double, c_double, P, c_size_t, P],
     "adx_loglik_workspace_bytes": [I64, I64, c_int, c_int, P],
     "adx_loglik": [P, I64, I64, c_int, c_int, P, P, P, P, c_size_t, P],
+    "adx_loglik_noalloc": [P, I64, I64, c_int, c_int, P, P, P, P],
 }
 _RESTYPE = {"adx_version": ctypes.c_char_p, "adx_last_error": ctypes.c_char_p}
 

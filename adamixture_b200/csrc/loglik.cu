@@ -13,6 +13,9 @@
 #include "common.cuh"
 
 #include <math.h>
+#include <stdio.h>
+
+#include <mutex>
 
 namespace adx {
 
@@ -197,6 +200,82 @@ extern "C" int adx_loglik(const uint8_t* G, int64_t M, int64_t N, int K, int pre
   if (precision == ADX_F64) { ADX_LL_KMAX_SWITCH(pl.kmax, L64) } else { ADX_LL_KMAX_SWITCH(pl.kmax, L32) }
 #undef L64
 #undef L32
+  ADX_LAUNCH_CHECK();
+  sum_partials_kernel<<<1, 256, 0, st>>>(part, nblk, out);
+  ADX_LAUNCH_CHECK();
+  return ADX_OK;
+}
+
+// ---------------------------------------------------------------- allocation-free variant
+//
+// adx_loglik_noalloc: the same log-likelihood for callers that cannot allocate device
+// memory. Typical ones: a host whose device memory is owned by another allocator (a
+// framework pool or a language runtime that must account for every byte), and code
+// paths where the implicit device-wide synchronisation of cudaMalloc/cudaFree is not
+// acceptable. adx_loglik needs a small caller-provided workspace for its per-block
+// partial sums; this variant keeps them in a file-scope device array instead.
+//
+// Limit: the array holds ADX_LL_NOALLOC_MAX_PARTIALS float64 partial sums (16 KiB) on every
+// GPU that loads the library, until the process exits. The launch plan uses fewer than
+// 1200 partials for any M, N and K (LL_BLOCKS rounded up to a multiple of the split
+// count), so every problem size fits; a plan that needed more would be rejected with
+// ADX_ERR_WORKSPACE.
+//
+// Set-up: host code cannot use the array's name as a device address (it names a host-side
+// stand-in). The first call on each device, with that device current, looks the address
+// up with cudaGetSymbolAddress and caches it; make that first call before any stream
+// capture begins. The array is shared by every call and keeps the previous call's
+// contents; each call overwrites every partial it reads, so nothing needs clearing. Two
+// calls whose launches overlap on the GPU (different streams, no ordering) race on it.
+
+#define ADX_LL_NOALLOC_MAX_PARTIALS 2048
+
+static __device__ __align__(256) double g_ll_noalloc_partials[ADX_LL_NOALLOC_MAX_PARTIALS];
+
+static std::mutex g_ll_noalloc_mu;
+static double* g_ll_noalloc_ptr[256];
+
+static int ll_noalloc_scratch(double** out) {
+  int dev = -1;
+  ADX_CUDA_TRY(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 256) { adx_set_message("adx_loglik_noalloc: device index out of range"); return ADX_ERR_ARG; }
+  std::lock_guard<std::mutex> lock(g_ll_noalloc_mu);
+  if (!g_ll_noalloc_ptr[dev]) {
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_ll_noalloc_partials);
+    if (e != cudaSuccess || !p) {
+      adx_set_cuda_error(e != cudaSuccess ? e : cudaErrorInvalidSymbol);
+      return ADX_ERR_CUDA;
+    }
+    g_ll_noalloc_ptr[dev] = static_cast<double*>(p);
+  }
+  *out = g_ll_noalloc_ptr[dev];
+  return ADX_OK;
+}
+
+extern "C" int adx_loglik_noalloc(const uint8_t* G, int64_t M, int64_t N, int K, int precision,
+                                  const void* P, const void* Q, double* out, void* stream) {
+  LlPlan pl;
+  int rc = ll_plan(M, N, K, precision, pl);
+  if (rc) { adx_set_message("adx_loglik_noalloc: bad shape or precision"); return rc; }
+  if (!G || !P || !Q || !out) { adx_set_message("adx_loglik_noalloc: null pointer"); return ADX_ERR_ARG; }
+  const int nblk = pl.n_split * pl.n_mblk;
+  if (nblk > ADX_LL_NOALLOC_MAX_PARTIALS) {
+    char msg[160];
+    snprintf(msg, sizeof(msg), "adx_loglik_noalloc: plan needs %d partial sums, the static scratch holds %d",
+             nblk, ADX_LL_NOALLOC_MAX_PARTIALS);
+    adx_set_message(msg);
+    return ADX_ERR_WORKSPACE;
+  }
+  double* part = nullptr;
+  rc = ll_noalloc_scratch(&part);
+  if (rc) return rc;
+  cudaStream_t st = as_stream(stream);
+#define N64(KM) loglik_kernel<double, KM><<<nblk, LL_TPB, 0, st>>>(G, (const double*)P, (const double*)Q, M, N, K, pl.n_stile, pl.n_split, pl.n_mblk, pl.mb, part)
+#define N32(KM) loglik_kernel<float, KM><<<nblk, LL_TPB, 0, st>>>(G, (const float*)P, (const float*)Q, M, N, K, pl.n_stile, pl.n_split, pl.n_mblk, pl.mb, part)
+  if (precision == ADX_F64) { ADX_LL_KMAX_SWITCH(pl.kmax, N64) } else { ADX_LL_KMAX_SWITCH(pl.kmax, N32) }
+#undef N64
+#undef N32
   ADX_LAUNCH_CHECK();
   sum_partials_kernel<<<1, 256, 0, st>>>(part, nblk, out);
   ADX_LAUNCH_CHECK();
