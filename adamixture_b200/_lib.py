@@ -13,7 +13,7 @@ from pathlib import Path
 
 LIB_PATH = Path(__file__).resolve().parent / "_lib" / "libadamixture_b200.so"
 
-ADX_OK, ADX_ERR_ARG, ADX_ERR_CUDA, ADX_ERR_WORKSPACE, ADX_ERR_UNSUPPORTED = 0, 1, 2, 3, 4
+ADX_OK, ADX_ERR_ARG, ADX_ERR_CUDA, ADX_ERR_WORKSPACE, ADX_ERR_UNSUPPORTED, ADX_ERR_TIMEOUT = 0, 1, 2, 3, 4, 5
 ADX_F64, ADX_F32, ADX_BF16 = 0, 1, 2
 MAX_K = 64
 
@@ -32,6 +32,7 @@ SIGNATURES: dict[str, list] = {
     "adx_bed_to_packed": [P, I64, I64, P, P, P, c_size_t, P],
     "adx_simulate_packed": [P, P, I64, I64, c_int, c_uint64, c_uint64, c_uint32, P, P],
     "adx_em_workspace_bytes": [I64, I64, c_int, c_int, P],
+    "adx_em_status": [P, c_size_t, I64, I64, c_int, c_int, P, P],
     "adx_em_stats": [P, I64, I64, c_int, c_int, P, P, P, P, P, P, c_size_t, P],
     "adx_em_sweep": [P, I64, I64, c_int, c_int, P, P, P, c_size_t, P],
     "adx_em_targets": [P, P, P, P, P, P, I64, I64, c_int, P, P, P],

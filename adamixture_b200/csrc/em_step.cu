@@ -52,7 +52,10 @@ struct EmPlan {
   int n_mblk;        // SNP blocks (partials of T)
   int64_t mb;        // SNPs per SNP block
   size_t ab_elems, t_elems, elem_size;
-  size_t bytes() const { return (ab_elems + t_elems) * elem_size + 256; }
+  // Workspace: a 256-byte header whose first word is the sweep's sticky status (the same
+  // offset for every shape, so a shared grow-only buffer keeps it), then the partials.
+  static constexpr size_t HEADER = 256;
+  size_t bytes() const { return HEADER + (ab_elems + t_elems) * elem_size; }
 };
 
 // ---------------------------------------------------------------- device helpers
@@ -341,11 +344,30 @@ static void cfg_of(int& W, int& CH) {
     default: break;                                                                    \
   }
 
+int tc_plan(int64_t M, int64_t N, int K, int64_t& n_stile, int& n_split, int& n_mblk);
+int tc_sweep(const uint8_t* G, const float* P, const float* Q, int64_t M, int64_t N, int K,
+             int64_t n_stile, int n_split, int n_mblk, float* ABp, float* Tp, int* err,
+             cudaStream_t st);
+
 int em_plan(int64_t M, int64_t N, int K, int prec, EmPlan& pl) {
   if (M <= 0 || N <= 0 || K < 1 || K > ADX_MAX_K) return ADX_ERR_ARG;
-  if (prec != ADX_F64 && prec != ADX_F32) return ADX_ERR_UNSUPPORTED;
+  if (prec != ADX_F64 && prec != ADX_F32 && prec != ADX_BF16) return ADX_ERR_UNSUPPORTED;
   pl.M = M; pl.N = N; pl.K = K; pl.prec = prec;
   pl.kmax = pick_kmax(K);
+  if (prec == ADX_BF16) {
+    // tensor-core sweep: 896-SNP blocks x 128-sample tiles, float partials
+    int64_t n_stile = 0;
+    int n_split = 0, n_mblk = 0;
+    const int rc = tc_plan(M, N, K, n_stile, n_split, n_mblk);
+    if (rc) return rc;
+    pl.W = 128; pl.CH = 0;
+    pl.elem_size = sizeof(float);
+    pl.n_stile = n_stile; pl.n_split = n_split; pl.n_mblk = n_mblk;
+    pl.mb = 896;
+    pl.ab_elems = (size_t)n_split * (size_t)M * 2 * K;
+    pl.t_elems = (size_t)n_mblk * (size_t)N * K;
+    return ADX_OK;
+  }
   int W = 0, CH = 0;
 #define CFG64(KM) cfg_of<double, KM>(W, CH)
 #define CFG32(KM) cfg_of<float, KM>(W, CH)
@@ -376,7 +398,7 @@ int em_plan(int64_t M, int64_t N, int K, int prec, EmPlan& pl) {
 template <typename R>
 static int launch_sweep(const EmPlan& pl, const uint8_t* G, const void* P, const void* Q, void* ws,
                         cudaStream_t st) {
-  R* ABp = reinterpret_cast<R*>(ws);
+  R* ABp = reinterpret_cast<R*>(reinterpret_cast<uint8_t*>(ws) + EmPlan::HEADER);
   R* Tp = ABp + pl.ab_elems;
   const dim3 grid((unsigned)(pl.n_split * pl.n_mblk));
 #define LAUNCH(KM)                                                                              \
@@ -393,7 +415,7 @@ static int launch_update(const EmPlan& pl, void* ws, int mode, double* A, double
                          const double* q_bat, double* P, double* Q, float* P32, float* Q32,
                          double* mP, double* vP, double* mQ, double* vQ, AdamArgs ad,
                          cudaStream_t st) {
-  const R* ABp = reinterpret_cast<const R*>(ws);
+  const R* ABp = reinterpret_cast<const R*>(reinterpret_cast<const uint8_t*>(ws) + EmPlan::HEADER);
   const R* Tp = ABp + pl.ab_elems;
   const int threads = 128;
   const dim3 grid((unsigned)ceil_div(pl.M + pl.N, threads));
@@ -409,6 +431,12 @@ static int launch_update(const EmPlan& pl, void* ws, int mode, double* A, double
 
 int em_sweep(const EmPlan& pl, const uint8_t* G, const void* P, const void* Q, void* ws,
              cudaStream_t st) {
+  if (pl.prec == ADX_BF16) {
+    float* ABp = reinterpret_cast<float*>(reinterpret_cast<uint8_t*>(ws) + EmPlan::HEADER);
+    int* err = reinterpret_cast<int*>(ws);
+    return tc_sweep(G, (const float*)P, (const float*)Q, pl.M, pl.N, pl.K, pl.n_stile, pl.n_split,
+                    pl.n_mblk, ABp, ABp + pl.ab_elems, err, st);
+  }
   return pl.prec == ADX_F64 ? launch_sweep<double>(pl, G, P, Q, ws, st)
                             : launch_sweep<float>(pl, G, P, Q, ws, st);
 }
@@ -492,6 +520,21 @@ extern "C" int adx_em_workspace_bytes(int64_t M, int64_t N, int K, int precision
   const int rc = em_plan(M, N, K, precision, pl);
   if (rc) { adx_set_message("adx_em_workspace_bytes: bad shape or precision"); return rc; }
   *bytes = pl.bytes();
+  return ADX_OK;
+}
+
+extern "C" int adx_em_status(void* workspace, size_t workspace_bytes, int64_t M, int64_t N, int K,
+                             int precision, int* status, void* stream) {
+  EmPlan pl;
+  int rc = em_plan(M, N, K, precision, pl);
+  if (rc) { adx_set_message("adx_em_status: bad shape or precision"); return rc; }
+  if (!workspace || !status) { adx_set_message("adx_em_status: null pointer"); return ADX_ERR_ARG; }
+  if (workspace_bytes < pl.bytes()) { adx_set_message("adx_em_status: workspace too small"); return ADX_ERR_WORKSPACE; }
+  cudaStream_t st = as_stream(stream);
+  int* word = reinterpret_cast<int*>(workspace);
+  ADX_CUDA_TRY(cudaMemcpyAsync(status, word, sizeof(int), cudaMemcpyDeviceToHost, st));
+  ADX_CUDA_TRY(cudaStreamSynchronize(st));
+  ADX_CUDA_TRY(cudaMemsetAsync(word, 0, sizeof(int), st));
   return ADX_OK;
 }
 

@@ -11,7 +11,8 @@ the arithmetic.
 E-step arithmetic (``precision``): ``"f64"`` reproduces the reference's float64 path;
 ``"f32"`` forms ratios and partial sums in float32 (float64 cross-block sums);
 ``"bf16"`` is the tensor-core form for K >= 8. ``set_precision`` sets the default
-(environment: ``ADX_PRECISION``); the default policy is ``"f32"``.
+(environment: ``ADX_PRECISION``); the default policy ("auto") is ``"bf16"`` for
+8 <= K <= 16 and ``"f32"`` otherwise.
 """
 from __future__ import annotations
 
@@ -36,10 +37,17 @@ def set_precision(p: str) -> None:
     _PRECISION = p
 
 
+TC_MIN_K, TC_MAX_K = 8, 16
+
+
 def resolve_precision(K: int, precision: str | None = None) -> str:
+    """The E-step arithmetic for this K. "auto": tensor cores (BF16 operands, FP32
+    accumulation) for 8 <= K <= 16, float32 otherwise."""
     p = precision or _PRECISION
     if p == "auto":
-        return "f32"
+        return "bf16" if TC_MIN_K <= K <= TC_MAX_K else "f32"
+    if p == "bf16" and K > TC_MAX_K:
+        raise ValueError(f"the tensor-core E-step supports K <= {TC_MAX_K} (got K={K}); use 'f32'")
     return p
 
 
@@ -171,8 +179,13 @@ def _optimize_parameters_gpu_once(G, P, Q, lr, beta1, beta2, reg_adam, max_iter,
 
     def loglik():
         if ll_prec == "f64":
-            return float(ops.loglik_device(G, P, Q, M, "f64").item())
-        return float(ops.loglik_device(G, P32, Q32, M, "f32").item())
+            L = float(ops.loglik_device(G, P, Q, M, "f64").item())
+        else:
+            L = float(ops.loglik_device(G, P32, Q32, M, "f32").item())
+        st = ops.em_status(ws, M, N, K, prec)
+        if st:
+            raise RuntimeError(f"E-step sweep reported status {st} (a bounded wait timed out)")
+        return L
 
     ts = time.time()
     opt.fused_iteration(G, P, Q, P32, Q32, M, ws)

@@ -60,7 +60,8 @@ class Workspace:
         buf = cls._bufs.get(key)
         if buf is None or buf.numel() < nbytes:
             cls._bufs[key] = None
-            buf = torch.empty(max(nbytes, 256), dtype=torch.uint8, device=device)
+            # zero-filled: the E-step workspace ends with a sticky status word
+            buf = torch.zeros(max(nbytes, 256), dtype=torch.uint8, device=device)
             cls._bufs[key] = buf
         return buf
 
@@ -160,6 +161,17 @@ def em_stats(G: torch.Tensor, P: torch.Tensor, Q: torch.Tensor, M: int, precisio
     call("adx_em_stats", G.data_ptr(), M, N, K, pc, P.data_ptr(), Q.data_ptr(), A.data_ptr(),
          B.data_ptr(), T.data_ptr(), ws.data_ptr(), ws.numel(), _stream(dev))
     return A, B, T
+
+
+def em_status(workspace: torch.Tensor, M: int, N: int, K: int, precision) -> int:
+    """Read and clear the sweep status word of ``workspace`` (0 = ok, 5 = a bounded
+    in-kernel wait timed out). Synchronises the current stream."""
+    import ctypes
+
+    out = ctypes.c_int(0)
+    call("adx_em_status", workspace.data_ptr(), workspace.numel(), M, N, K,
+         precision_code(precision), ctypes.addressof(out), _stream(workspace.device))
+    return int(out.value)
 
 
 def em_sweep(G: torch.Tensor, P: torch.Tensor, Q: torch.Tensor, M: int, precision,

@@ -289,7 +289,7 @@ def run_gpu_arm(args, cfg, rank, world, local_rank):
     achieved = ab / (sweep_ms * 1e-3) / 1e9
     roof = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
             "frac": achieved / hbm, "traffic": traffic_per_launch(M, N, K, prec),
-            "kernel": f"em_sweep_kernel<{'double' if prec == 'f64' else 'float'},{ops_kmax(K)}>",
+            "kernel": "em_sweep_tc_kernel" if prec == "bf16" else f"em_sweep_kernel<{'double' if prec == 'f64' else 'float'},{ops_kmax(K)}>",
             "launch_ms": sweep_ms, "alg_bytes": ab, "peak_kind": peak_kind,
             "entries_per_s": M * N / (sweep_ms * 1e-3)}
 

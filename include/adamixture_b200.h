@@ -12,8 +12,8 @@
  *    (The reference's GPU layout, adamixture/src/utils_c/cython/snp_reader.pyx:76-120.)
  *  - P is [M][K], Q is [N][K], row-major. "precision" selects the E-step arithmetic:
  *    ADX_F64 (float64, the reference GPU path's precision), ADX_F32, ADX_BF16
- *    (tensor-core form, K >= 8). P/Q passed to a pass are double for ADX_F64 and float
- *    otherwise.
+ *    (tcgen05 tensor-core form with BF16 operands and FP32 accumulation, K <= 16). P/Q
+ *    passed to a pass are double for ADX_F64 and float otherwise.
  *  - Calls that need scratch memory take a caller-allocated `workspace` whose size
  *    adx_*_workspace_bytes() reports; none of them allocates device memory.
  */
@@ -33,6 +33,7 @@ enum {
   ADX_ERR_CUDA = 2,         /* a CUDA runtime call or launch failed */
   ADX_ERR_WORKSPACE = 3,    /* workspace smaller than adx_*_workspace_bytes() */
   ADX_ERR_UNSUPPORTED = 4,  /* precision/K combination not built */
+  ADX_ERR_TIMEOUT = 5,      /* a bounded in-kernel wait gave up (reported by adx_em_status) */
 };
 
 enum { ADX_F64 = 0, ADX_F32 = 1, ADX_BF16 = 2 };
@@ -84,8 +85,15 @@ int adx_simulate_packed(const uint32_t* Pq, const uint32_t* Qq, int64_t M, int64
 
 /* ---------------------------------------------------------------- Adam-EM */
 
-/* Scratch needed by adx_em_stats / adx_em_adam_iteration for this shape. */
+/* Scratch needed by adx_em_stats / adx_em_sweep / adx_em_adam_iteration for this shape.
+ * Zero-fill it once after allocating: its first word is a sticky status word (the same
+ * offset for every shape, so one buffer can serve several shapes). */
 int adx_em_workspace_bytes(int64_t M, int64_t N, int K, int precision, size_t* bytes);
+
+/* Read and clear the workspace's status word (ADX_OK, or ADX_ERR_TIMEOUT when a sweep's
+ * bounded wait for its tensor-core work gave up). Synchronises `stream`. */
+int adx_em_status(void* workspace, size_t workspace_bytes, int64_t M, int64_t N, int K,
+                  int precision, int* status, void* stream);
 
 /* One fused E-step sweep over G: A, B [M][K] and T [N][K] (float64), the sufficient
  * statistics EMAdamOptimizer.run_em_step accumulates (A_accum, B_accum, T_accum;
