@@ -54,8 +54,11 @@ struct EmPlan {
   size_t ab_elems, t_elems, elem_size;
   // Workspace: a 256-byte header whose first word is the sweep's sticky status (the same
   // offset for every shape, so a shared grow-only buffer keeps it), then the partials.
+  // The tensor-core sweep also keeps a BF16 copy of Q after the partials.
   static constexpr size_t HEADER = 256;
-  size_t bytes() const { return HEADER + (ab_elems + t_elems) * elem_size; }
+  size_t extra_bytes = 0;
+  size_t extra_offset() const { return (HEADER + (ab_elems + t_elems) * elem_size + 255) & ~size_t(255); }
+  size_t bytes() const { return extra_offset() + extra_bytes; }
 };
 
 // ---------------------------------------------------------------- device helpers
@@ -345,8 +348,9 @@ static void cfg_of(int& W, int& CH) {
   }
 
 int tc_plan(int64_t M, int64_t N, int K, int64_t& n_stile, int& n_split, int& n_mblk);
+size_t tc_q_bytes(int64_t n_stile);
 int tc_sweep(const uint8_t* G, const float* P, const float* Q, int64_t M, int64_t N, int K,
-             int64_t n_stile, int n_split, int n_mblk, float* ABp, float* Tp, int* err,
+             int64_t n_stile, int n_split, int n_mblk, float* ABp, float* Tp, void* Qb, int* err,
              cudaStream_t st);
 
 int em_plan(int64_t M, int64_t N, int K, int prec, EmPlan& pl) {
@@ -366,6 +370,7 @@ int em_plan(int64_t M, int64_t N, int K, int prec, EmPlan& pl) {
     pl.mb = 896;
     pl.ab_elems = (size_t)n_split * (size_t)M * 2 * K;
     pl.t_elems = (size_t)n_mblk * (size_t)N * K;
+    pl.extra_bytes = tc_q_bytes(n_stile);
     return ADX_OK;
   }
   int W = 0, CH = 0;
@@ -434,8 +439,9 @@ int em_sweep(const EmPlan& pl, const uint8_t* G, const void* P, const void* Q, v
   if (pl.prec == ADX_BF16) {
     float* ABp = reinterpret_cast<float*>(reinterpret_cast<uint8_t*>(ws) + EmPlan::HEADER);
     int* err = reinterpret_cast<int*>(ws);
+    void* Qb = reinterpret_cast<uint8_t*>(ws) + pl.extra_offset();
     return tc_sweep(G, (const float*)P, (const float*)Q, pl.M, pl.N, pl.K, pl.n_stile, pl.n_split,
-                    pl.n_mblk, ABp, ABp + pl.ab_elems, err, st);
+                    pl.n_mblk, ABp, ABp + pl.ab_elems, Qb, err, st);
   }
   return pl.prec == ADX_F64 ? launch_sweep<double>(pl, G, P, Q, ws, st)
                             : launch_sweep<float>(pl, G, P, Q, ws, st);

@@ -6,7 +6,7 @@
 // For each step (sample tile s, SNP tile r), in two half-steps of 64 samples:
 //   H  = P_r  . Q_s^T      (tcgen05.mma M=128 SNPs, N=64 samples, K=16)         -> TMEM
 //   Hc = (1-P_r) . Q_s^T   (the complement, so 1-h stays accurate when h -> 1)  -> TMEM
-//   8 warps read H/Hc rows from TMEM and form, per entry (one reciprocal each),
+//   consumer warps read H/Hc rows from TMEM and form, per entry (one reciprocal each),
 //     a = g / max(h,1e-5),  b = (2-g) / max(1-h,1e-5)   (0 where missing)
 //   as BF16 tiles in shared memory; after both halves
 //   A_r += a . Q_s, B_r += b . Q_s   (M=128 SNPs, N=16, K=128 samples; TMEM, all sample tiles)
@@ -14,14 +14,16 @@
 // After the R SNP tiles of a sample tile, T (over the CTA's 896 SNPs) goes to the T partials;
 // after the last sample tile, A_r/B_r go to the A/B partials of the CTA's split.
 //
-// Warp specialisation (9 warps): warpgroup 0 (warps 0-3) forms the ratios of the first 64
-// samples of every step, warpgroup 1 (warps 4-7) those of the second 64, and warp 8 is the
-// producer: it issues every MMA from one thread and streams the G tiles into shared memory
-// with cp.async. H/Hc live in two TMEM buffers (one per warpgroup) and the a/b tiles in two
-// shared-memory buffers (one per step parity), so while a warpgroup forms the ratios of
-// its half-step the tensor pipe runs the other warpgroup's H and the A/B/T MMAs of the
-// previous step. Q tiles are triple-buffered. There is no block-wide barrier in the loop:
-// the warps meet only at mbarriers.
+// Warp specialisation: HALF_WGS warpgroups form the ratios of the first 64 samples of every
+// step and as many those of the second 64 (each warpgroup a block of WG_COLS samples); the
+// last warp is the producer. Its lane 0 issues every MMA from precomputed shared-memory
+// descriptors (a step's 34 MMAs cost one 64-bit add per operand), and the warp streams the
+// G tiles (a ring of NG stages, NG-1 steps ahead) and the BF16 Q tiles (NQ buffers, one
+// sample tile ahead) into shared memory with cp.async. H/Hc live in two TMEM buffers (one
+// per half) and the a/b tiles in two shared-memory buffers (one per step parity), so while
+// one half's warpgroups form their ratios the tensor pipe runs the other half's H and the
+// A/B/T MMAs of the previous step. There is no block-wide barrier in the loop: the warps
+// meet only at mbarriers, and loop counters advance incrementally (no division).
 //
 // TMEM (512 columns, one CTA per SM): H/Hc buffer b at [128b, 128b+128) (H first 64, Hc
 // last 64) | T [256,272) | A_r,B_r [272+32r, 304+32r) for r < 7.
@@ -30,44 +32,61 @@
 // and the MN-major B of T; Q_s is the K-major B of H and the MN-major B of A/B; the a/b
 // tiles are the K-major A of A/B and the MN-major A of T.
 //
-// Synchronisation (mbarriers): hfull[w] (tcgen05.commit: H of warpgroup w's next half-step
-// and every MMA issued before it are done), abready[w] (128 arrivals: warpgroup w wrote its
-// a/b half and finished reading its H buffer), gfull[b] (32 arrivals from cp.async: G tile
-// buffer b is loaded). Every wait is bounded and also watches a shared abort word; on a
-// timeout the kernel records ADX_ERR_TIMEOUT in the status word, all warps leave their
-// loops, it waits (bounded) for its MMAs in flight, frees its TMEM and returns.
+// Synchronisation (mbarriers): hfull[h] (tcgen05.commit: H of half h's next half-step and
+// every MMA issued before it are done), abready[h] (128*HALF_WGS arrivals: half h's
+// warpgroups wrote their a/b columns and finished reading their H buffer), gfull[g] and
+// qfull[q] (32 cp.async arrivals: G stage g / Q buffer q is loaded). Every wait is bounded
+// and also watches a shared abort word; on a timeout the kernel records ADX_ERR_TIMEOUT in
+// the status word, all warps leave their loops, it waits (bounded) for its MMAs in flight,
+// frees its TMEM and returns.
 #include "common.cuh"
 
 #include <cuda_bf16.h>
 
+#ifndef ADX_TC_HALF_WGS
+#define ADX_TC_HALF_WGS 2
+#endif
+
 namespace adx {
 namespace tc {
 
-constexpr int TPB = 288;          // 2 consumer warpgroups + 1 producer warp
-constexpr int PRODUCER_WARP = 8;
 constexpr int TILE = 128;      // SNPs per SNP tile, samples per sample tile
 constexpr int KP = 16;         // padded K
 constexpr int R = 7;           // SNP tiles per CTA
 constexpr int SNP_BLOCK = R * TILE;
+constexpr int HALF = TILE / 2;                          // samples per half-step
+constexpr int HALF_WGS = ADX_TC_HALF_WGS;               // consumer warpgroups per half
+constexpr int WG_COLS = HALF / HALF_WGS;                // samples per warpgroup and half-step
+constexpr int CONSUMER_WARPS = 2 * 4 * HALF_WGS;
+constexpr int PRODUCER_WARP = CONSUMER_WARPS;
+constexpr int TPB = CONSUMER_WARPS * 32 + 32;
+constexpr int NG = 4;          // G stages
+constexpr int NQ = 3;          // Q buffers
+static_assert(WG_COLS % 16 == 0, "warpgroup column blocks are whole 16-column TMEM loads");
 
 // shared-memory map (bytes)
-constexpr int P_TILE_BYTES = TILE * KP * 2;             // 4096
-constexpr int OFF_P = 0;                                // R x (P, 1-P)
-constexpr int OFF_Q = OFF_P + R * 2 * P_TILE_BYTES;     // 3 buffers
-constexpr int OFF_G = OFF_Q + 3 * P_TILE_BYTES;         // 2 buffers x 32 rows x 128 bytes
-constexpr int G_TILE_BYTES = (TILE / 4) * TILE;         // 4096
-constexpr int OFF_A = OFF_G + 2 * G_TILE_BYTES;         // 2 buffers
+constexpr int P_TILE_BYTES = TILE * KP * 2;             // 4096 (also one Q tile)
+constexpr int G_ROW = TILE + 16;                        // padded packed row of a G tile
+constexpr int G_TILE_BYTES = (TILE / 4) * G_ROW;        // 32 packed rows
 constexpr int AB_TILE_BYTES = TILE * TILE * 2;          // 32768
+constexpr int OFF_P = 0;                                // R x (P, 1-P)
+constexpr int OFF_Q = OFF_P + R * 2 * P_TILE_BYTES;     // NQ buffers
+constexpr int OFF_G = OFF_Q + NQ * P_TILE_BYTES;        // NG stages
+constexpr int OFF_A = OFF_G + NG * G_TILE_BYTES;        // 2 buffers
 constexpr int OFF_B = OFF_A + 2 * AB_TILE_BYTES;        // 2 buffers
-constexpr int OFF_BAR = OFF_B + 2 * AB_TILE_BYTES;      // 6 mbarriers
-constexpr int OFF_TMEM = OFF_BAR + 48;                  // TMEM address, then the abort word
+constexpr int OFF_BAR = OFF_B + 2 * AB_TILE_BYTES;      // mbarriers
+constexpr int N_BARS = 2 + 2 + NG + NQ;
+constexpr int OFF_TMEM = OFF_BAR + 8 * N_BARS;          // TMEM address, then the abort word
 constexpr int SMEM_BYTES = OFF_TMEM + 16;
 constexpr int SMEM_ALLOC = SMEM_BYTES + 1024;           // room to align the base to 1024
 static_assert(SMEM_ALLOC <= 227 * 1024, "shared memory budget");
+static_assert(OFF_G % 16 == 0 && G_TILE_BYTES % 16 == 0 && G_ROW % 16 == 0, "cp.async alignment");
+// descriptor start addresses are 14-bit fields of 16-byte units: offsets added to a base
+// descriptor never carry out of the field while the whole map stays below 256 KiB
+static_assert(SMEM_ALLOC < 256 * 1024, "descriptor start field");
 
 // TMEM columns
 constexpr uint32_t COL_T = 256, COL_AB = 272;
-constexpr int HALF = TILE / 2;                          // samples per half-step
 
 constexpr uint32_t WAIT_LIMIT = 1u << 26;  // ~seconds of polling before giving up
 
@@ -201,7 +220,7 @@ constexpr uint32_t GB_LO = 0x3F804000u, GB_HI = 0x00000000u;  // g -> {2, 1, 0, 
 struct Args {
   const uint8_t* G;
   const float* P;     // [M][K] float32
-  const float* Q;     // [N][K] float32
+  const uint8_t* Qb;  // BF16 Q tiles [n_stile][4096 B], shared-memory layout
   int64_t M, N;
   int K;
   int64_t n_stile;    // sample tiles
@@ -212,16 +231,35 @@ struct Args {
   int* err;
 };
 
-// G tile (32 packed rows x 128 samples) into shared memory by the producer warp: lane l
-// copies row l. Whole 16-byte chunks go by cp.async and the lane's arrival on `bar` fires
+// Q (float32 [N][K]) -> BF16 tiles of 128 samples x 16 in the shared-memory layout of a Q
+// tile (rows past N and columns past K are zero), so the producer copies them verbatim.
+__global__ void q_to_bf16_kernel(const float* __restrict__ Q, int64_t N, int K, int64_t n_stile,
+                                 uint8_t* __restrict__ Qb) {
+  const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= n_stile * TILE * 2) return;
+  const int64_t tile = e / (TILE * 2);
+  const int row = (int)((e >> 1) % TILE), kh = (int)(e & 1) * 8;
+  const int64_t i = tile * TILE + row;
+  float f[8];
+#pragma unroll
+  for (int q = 0; q < 8; ++q) {
+    const int k = kh + q;
+    f[q] = (i < N && k < K) ? __ldg(Q + i * K + k) : 0.0f;
+  }
+  *reinterpret_cast<uint4*>(Qb + tile * P_TILE_BYTES + off_pq(row, kh)) =
+      make_uint4(pack_bf16x2(f[0], f[1]), pack_bf16x2(f[2], f[3]), pack_bf16x2(f[4], f[5]), pack_bf16x2(f[6], f[7]));
+}
+
+// G tile (32 packed rows x 128 samples) into a shared-memory stage by the producer warp: lane
+// l copies row l. Whole 16-byte chunks go by cp.async and the lane's arrival on `bar` fires
 // when they land; rows that end past N, or a sample count that is not a multiple of 16,
-// take byte loads and a plain arrival.
+// take byte loads (0xFF, all missing, past the ends) and a plain arrival.
 __device__ __forceinline__ void producer_load_g(const Args& a, int64_t row0, int64_t i0, bool vec16,
                                                 uint8_t* gs, uint32_t bar) {
   const int l = threadIdx.x & 31;
   const int64_t row = row0 + l;
   const int64_t rows = (a.M + 3) >> 2;
-  uint8_t* dst = gs + l * TILE;
+  uint8_t* dst = gs + l * G_ROW;
   if (row < rows && vec16 && i0 + TILE <= a.N) {
     const uint8_t* src = a.G + row * a.N + i0;
 #pragma unroll
@@ -242,22 +280,14 @@ __device__ __forceinline__ void producer_load_g(const Args& a, int64_t row0, int
   }
 }
 
-// Q tile (128 samples x 16, bf16) by the producer warp: lane l converts samples 4l..4l+3.
-__device__ __forceinline__ void producer_load_q(const Args& a, int64_t i0, uint8_t* qs) {
+// BF16 Q tile (4096 B) into a shared-memory buffer by the producer warp: lane l copies
+// bytes [128 l, 128 l + 128).
+__device__ __forceinline__ void producer_load_q(const Args& a, int64_t tile, uint8_t* qs, uint32_t bar) {
   const int l = threadIdx.x & 31;
-#pragma unroll 1
-  for (int e = 0; e < 8; ++e) {
-    const int row = l * 4 + (e >> 1), kh = (e & 1) * 8;
-    const int64_t i = i0 + row;
-    float f[8];
+  const uint8_t* src = a.Qb + tile * P_TILE_BYTES + l * 128;
 #pragma unroll
-    for (int q = 0; q < 8; ++q) {
-      const int k = kh + q;
-      f[q] = (i < a.N && k < a.K) ? __ldg(a.Q + i * a.K + k) : 0.0f;
-    }
-    *reinterpret_cast<uint4*>(qs + off_pq(row, kh)) =
-        make_uint4(pack_bf16x2(f[0], f[1]), pack_bf16x2(f[2], f[3]), pack_bf16x2(f[4], f[5]), pack_bf16x2(f[6], f[7]));
-  }
+  for (int c = 0; c < 8; ++c) cp_async16(smem_u32(qs + l * 128 + 16 * c), src + 16 * c);
+  cp_async_arrive(bar);
 }
 
 __global__ void __launch_bounds__(TPB, 1) em_sweep_tc_kernel(Args a) {
@@ -266,9 +296,10 @@ __global__ void __launch_bounds__(TPB, 1) em_sweep_tc_kernel(Args a) {
   uint32_t* tmem_holder = reinterpret_cast<uint32_t*>(sm + OFF_TMEM);
   volatile int* abort_flag = reinterpret_cast<volatile int*>(sm + OFF_TMEM + 4);
   const uint32_t bars = smem_u32(sm + OFF_BAR);
-  auto HFULL = [&](int w) { return bars + 8u * (uint32_t)w; };
-  auto ABREADY = [&](int w) { return bars + 16u + 8u * (uint32_t)w; };
-  auto GFULL = [&](int b) { return bars + 32u + 8u * (uint32_t)b; };
+  auto HFULL = [&](int h) { return bars + 8u * (uint32_t)h; };
+  auto ABREADY = [&](int h) { return bars + 16u + 8u * (uint32_t)h; };
+  auto GFULL = [&](int g) { return bars + 32u + 8u * (uint32_t)g; };
+  auto QFULL = [&](int q) { return bars + 32u + 8u * (uint32_t)NG + 8u * (uint32_t)q; };
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
 
   const int mblk = blockIdx.x % a.n_mblk;
@@ -276,10 +307,9 @@ __global__ void __launch_bounds__(TPB, 1) em_sweep_tc_kernel(Args a) {
   const int64_t jb = (int64_t)mblk * SNP_BLOCK;
   const int r_eff = (int)min((int64_t)R, (a.M - jb + TILE - 1) / TILE);
   const int64_t s_first = split;
-  const int64_t n_my = (a.n_stile - split + a.n_split - 1) / a.n_split;  // sample tiles of this CTA
+  const int n_my = (int)((a.n_stile - split + a.n_split - 1) / a.n_split);  // sample tiles of this CTA
   const bool vec16 = (a.N & 15) == 0;
-  const int64_t nsteps = n_my * r_eff;
-  const int64_t nhalf = 2 * nsteps;
+  const int nsteps = n_my * r_eff;
 
   // ---- prologue: TMEM (producer warp), barriers, P tiles (all threads)
   if (warp == PRODUCER_WARP) {
@@ -288,12 +318,12 @@ __global__ void __launch_bounds__(TPB, 1) em_sweep_tc_kernel(Args a) {
   }
   if (tid == 0) {
     *abort_flag = 0;
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(HFULL(0)));
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(HFULL(1)));
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 128;" ::"r"(ABREADY(0)));
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 128;" ::"r"(ABREADY(1)));
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 32;" ::"r"(GFULL(0)));
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 32;" ::"r"(GFULL(1)));
+    for (int h = 0; h < 2; ++h) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(HFULL(h)));
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(ABREADY(h)), "r"(128 * HALF_WGS));
+    }
+    for (int g = 0; g < NG; ++g) asm volatile("mbarrier.init.shared::cta.b64 [%0], 32;" ::"r"(GFULL(g)));
+    for (int q = 0; q < NQ; ++q) asm volatile("mbarrier.init.shared::cta.b64 [%0], 32;" ::"r"(QFULL(q)));
     asm volatile("fence.mbarrier_init.release.cluster;");
   }
   for (int e = tid; e < r_eff * TILE * 2; e += TPB) {
@@ -319,43 +349,44 @@ __global__ void __launch_bounds__(TPB, 1) em_sweep_tc_kernel(Args a) {
   __syncthreads();
   fence_after();
   const uint32_t tmem = *tmem_holder;
-  const uint32_t s_p = smem_u32(sm + OFF_P), s_q = smem_u32(sm + OFF_Q);
-  const uint32_t s_a = smem_u32(sm + OFF_A), s_b = smem_u32(sm + OFF_B);
   const float ELO = (float)E_CLAMP;
 
-  // H/Hc of half-step u (step u/2, half u&1) into TMEM buffer u&1
-  auto issue_h = [&](int64_t u) {
-    const int64_t st = u >> 1;
-    const int r = (int)(st % r_eff);
-    const int qb = (int)((st / r_eff) % 3);
-    const int h = (int)(u & 1);
-    const uint32_t pa = s_p + r * 2 * P_TILE_BYTES;
-    const uint64_t bq = sdesc(s_q + qb * P_TILE_BYTES + h * (HALF / 8) * 256, 128, 256);
-    const uint32_t col = (uint32_t)h * 128;
-    mma_bf16(tmem + col, sdesc(pa, 128, 256), bq, ID_H, 0);
-    mma_bf16(tmem + col + HALF, sdesc(pa + P_TILE_BYTES, 128, 256), bq, ID_H, 0);
+  // Base descriptors; the offsets added below are in 16-byte units.
+  const uint32_t s_p = smem_u32(sm + OFF_P), s_q = smem_u32(sm + OFF_Q), s_a = smem_u32(sm + OFF_A);
+  const uint64_t dPK = sdesc(s_p, 128, 256);    // P_r K-major (A of H): + 512 r; 1-P: + 256
+  const uint64_t dQK = sdesc(s_q, 128, 256);    // Q K-major (B of H): + 256 qb + 128 half
+  const uint64_t dQM = sdesc(s_q, 256, 128);    // Q MN-major (B of A/B): + 256 qb + 32 ks
+  const uint64_t dAK = sdesc(s_a, 128, 2048);   // a K-major (A of A/B): + 2048 buf + 16 ks; b: + 4096
+  const uint64_t dAM = sdesc(s_a, 2048, 128);   // a MN-major (A of T): + 2048 buf + 256 ks; b: + 4096
+  const uint64_t dPM = sdesc(s_p, 256, 128);    // P_r MN-major (B of T): + 512 r + 32 ks; 1-P: + 256
+  constexpr uint64_t B_OFF = (uint64_t)(OFF_B - OFF_A) >> 4;
+
+  // H/Hc of half h of a step on SNP tile r and Q buffer qb, into TMEM buffer h
+  auto issue_h = [&](int r, int qb, int h) {
+    const uint64_t bq = dQK + (uint64_t)(qb * 256 + h * 128);
+    const uint64_t ap = dPK + (uint64_t)(r * 512);
+    const uint32_t col = tmem + (uint32_t)h * 128;
+    mma_bf16(col, ap, bq, ID_H, 0);
+    mma_bf16(col + HALF, ap + 256, bq, ID_H, 0);
   };
-  // A/B/T MMAs of step st (a/b buffer st&1)
-  auto issue_abt = [&](int64_t st) {
-    const int64_t sidx = st / r_eff;
-    const int r = (int)(st % r_eff);
-    const uint32_t sq = s_q + (int)(sidx % 3) * P_TILE_BYTES;
-    const uint32_t ta = s_a + (int)(st & 1) * AB_TILE_BYTES, tb = s_b + (int)(st & 1) * AB_TILE_BYTES;
-    const uint32_t acc_ab = (sidx > 0) ? 1u : 0u;
+  // A/B/T MMAs of a step on SNP tile r, Q buffer qb, a/b buffer buf
+  auto issue_abt = [&](int r, int qb, int buf, bool acc_ab) {
+    const uint64_t qm = dQM + (uint64_t)(qb * 256);
+    const uint64_t ak = dAK + (uint64_t)(buf * 2048);
+    const uint32_t tab = tmem + COL_AB + 32u * (uint32_t)r;
 #pragma unroll
     for (int ks = 0; ks < TILE / 16; ++ks) {
-      const uint64_t bq = sdesc(sq + ks * 2 * 256, 256, 128);
-      const uint32_t acc = (acc_ab | (ks > 0)) ? 1u : 0u;
-      mma_bf16(tmem + COL_AB + 32 * r, sdesc(ta + ks * 2 * 128, 128, 2048), bq, ID_AB, acc);
-      mma_bf16(tmem + COL_AB + 32 * r + 16, sdesc(tb + ks * 2 * 128, 128, 2048), bq, ID_AB, acc);
+      const uint32_t acc = (acc_ab || ks > 0) ? 1u : 0u;
+      mma_bf16(tab, ak + 16 * ks, qm + 32 * ks, ID_AB, acc);
+      mma_bf16(tab + 16, ak + B_OFF + 16 * ks, qm + 32 * ks, ID_AB, acc);
     }
-    const uint32_t pa = s_p + r * 2 * P_TILE_BYTES;
+    const uint64_t am = dAM + (uint64_t)(buf * 2048);
+    const uint64_t pm = dPM + (uint64_t)(r * 512);
 #pragma unroll
     for (int ks = 0; ks < TILE / 16; ++ks) {
       const uint32_t acc = (r > 0 || ks > 0) ? 1u : 0u;
-      mma_bf16(tmem + COL_T, sdesc(ta + ks * 2 * 2048, 2048, 128), sdesc(pa + ks * 2 * 256, 256, 128), ID_T, acc);
-      mma_bf16(tmem + COL_T, sdesc(tb + ks * 2 * 2048, 2048, 128),
-               sdesc(pa + P_TILE_BYTES + ks * 2 * 256, 256, 128), ID_T, 1u);
+      mma_bf16(tmem + COL_T, am + 256 * ks, pm + 32 * ks, ID_T, acc);
+      mma_bf16(tmem + COL_T, am + B_OFF + 256 * ks, pm + 256 + 32 * ks, ID_T, 1u);
     }
   };
   auto write_t = [&](int64_t s) {  // one warpgroup: T rows (samples) of sample tile s
@@ -374,83 +405,107 @@ __global__ void __launch_bounds__(TPB, 1) em_sweep_tc_kernel(Args a) {
   bool aborted = false;
   if (warp == PRODUCER_WARP) {
     // ---------------------------------------------------------------- producer
-    producer_load_q(a, s_first * TILE, sm + OFF_Q);
+    // Q of sample tile t goes to buffer t % NQ (k-th fill: parity k & 1), G of step g to
+    // stage g % NG; both are tracked by counters.
+    producer_load_q(a, s_first, sm + OFF_Q, QFULL(0));
+    if (n_my > 1) producer_load_q(a, s_first + a.n_split, sm + OFF_Q + P_TILE_BYTES, QFULL(1));
+    int gst = 0, gr = 0, gsidx = 0, gstage = 0;  // next G load: step, SNP tile, sample tile, stage
+    auto load_next_g = [&]() {
+      producer_load_g(a, (jb + (int64_t)gr * TILE) >> 2, (s_first + (int64_t)gsidx * a.n_split) * TILE,
+                      vec16, sm + OFF_G + gstage * G_TILE_BYTES, GFULL(gstage));
+      ++gst;
+      if (++gr == r_eff) { gr = 0; ++gsidx; }
+      if (++gstage == NG) gstage = 0;
+    };
+    while (gst < NG - 1 && gst < nsteps) load_next_g();
+    if (!mbar_wait(QFULL(0), 0u, abort_flag)) aborted = true;
     fence_async_smem();
-    __syncwarp();
-    producer_load_g(a, jb >> 2, s_first * TILE, vec16, sm + OFF_G, GFULL(0));
-    if (lane == 0) {
-      issue_h(0);
+    if (!aborted && lane == 0) {
+      issue_h(0, 0, 0);
       mma_commit(HFULL(0));
-      if (nhalf > 1) {
-        issue_h(1);
-        mma_commit(HFULL(1));
-      }
+      issue_h(0, 0, 1);
+      mma_commit(HFULL(1));
     }
     __syncwarp();
+    int r = 0, sidx = 0, qb = 0;       // the current step's SNP tile, sample tile, Q buffer
+    uint32_t qpar = 0u;                // parity of the Q buffer's fill for sample tile sidx
     uint32_t pab0 = 0u, pab1 = 0u;
-    for (int64_t u = 0; u < nhalf; ++u) {
-      const int w = (int)(u & 1);
-      const int64_t st = u >> 1;
-      if (!mbar_wait(ABREADY(w), w ? pab1 : pab0, abort_flag)) { aborted = true; break; }
-      if (w) pab1 ^= 1u; else pab0 ^= 1u;
+    for (int st = 0; st < nsteps && !aborted; ++st) {
+      int r1 = r + 1, sidx1 = sidx, qb1 = qb;
+      uint32_t qpar1 = qpar;
+      if (r1 == r_eff) {
+        r1 = 0;
+        ++sidx1;
+        if (++qb1 == NQ) { qb1 = 0; qpar1 ^= 1u; }
+      }
+      const bool more = st + 1 < nsteps;
+      // ---- half 0 of step st is formed: refill H buffer 0 with the next step's half 0
+      if (!mbar_wait(ABREADY(0), pab0, abort_flag)) { aborted = true; break; }
+      pab0 ^= 1u;
       fence_after();
-      // the next sample tile's Q must be in shared memory before its first H is issued
-      const int64_t un = u + 2;
-      if (un < nhalf && (un & 1) == 0 && ((un >> 1) % r_eff) == 0) {
-        const int64_t nsidx = (un >> 1) / r_eff;
-        producer_load_q(a, (s_first + nsidx * a.n_split) * TILE, sm + OFF_Q + (int)(nsidx % 3) * P_TILE_BYTES);
+      // at the first step of sample tile sidx >= 1, prefetch tile sidx + 1 into the buffer
+      // of tile sidx - 2, whose MMAs completed before this barrier phase
+      if (r == 0 && sidx >= 1 && sidx + 1 < n_my) {
+        const int qn = qb + 1 == NQ ? 0 : qb + 1;
+        producer_load_q(a, s_first + (int64_t)(sidx + 1) * a.n_split, sm + OFF_Q + qn * P_TILE_BYTES, QFULL(qn));
+      }
+      if (more && r1 == 0) {  // the next step starts a sample tile: its Q must have landed
+        if (!mbar_wait(QFULL(qb1), qpar1, abort_flag)) { aborted = true; break; }
         fence_async_smem();
-        __syncwarp();
       }
       if (lane == 0) {
-        if (w == 1) issue_abt(st);
-        if (un < nhalf) issue_h(un);
-        mma_commit(HFULL(w));
+        if (more) issue_h(r1, qb1, 0);
+        mma_commit(HFULL(0));
       }
       __syncwarp();
-      if (w == 0 && st + 1 < nsteps) {
-        const int nr = (int)((st + 1) % r_eff);
-        const int64_t ns = s_first + ((st + 1) / r_eff) * a.n_split;
-        producer_load_g(a, (jb + (int64_t)nr * TILE) >> 2, ns * TILE, vec16,
-                        sm + OFF_G + (int)((st + 1) & 1) * G_TILE_BYTES, GFULL((int)((st + 1) & 1)));
+      if (gst < nsteps) load_next_g();  // step st + NG - 1 into the stage step st - 1 used
+      // ---- half 1 of step st is formed: A/B/T of step st, then the next step's half 1
+      if (!mbar_wait(ABREADY(1), pab1, abort_flag)) { aborted = true; break; }
+      pab1 ^= 1u;
+      fence_after();
+      if (lane == 0) {
+        issue_abt(r, qb, st & 1, sidx > 0);
+        if (more) issue_h(r1, qb1, 1);
+        mma_commit(HFULL(1));
       }
+      __syncwarp();
+      r = r1; sidx = sidx1; qb = qb1; qpar = qpar1;
     }
   } else {
     // ---------------------------------------------------------------- consumers
-    const int w = warp >> 2;           // warpgroup = half of every step
-    const int wq = warp & 3;           // TMEM lane quarter
-    const int jl = wq * 32 + lane;     // SNP row within the tile
-    const uint32_t trow = tmem + ((uint32_t)(wq * 32) << 16) + (uint32_t)w * 128;
+    const int hw = warp / (4 * HALF_WGS);       // half of every step
+    const int sub = (warp >> 2) % HALF_WGS;     // column block inside the half
+    const int wq = warp & 3;                    // TMEM lane quarter
+    const int jl = wq * 32 + lane;              // SNP row within the tile
+    const int colb = hw * HALF + sub * WG_COLS; // first sample column inside the step's tile
+    const uint32_t trow = tmem + ((uint32_t)(wq * 32) << 16) + (uint32_t)(hw * 128 + sub * WG_COLS);
     const uint32_t sh = 2u * (uint32_t)(jl & 3);
-    uint32_t ph = 0u;
-    for (int64_t u = w; u < nhalf; u += 2) {
-      const int64_t st = u >> 1;
-      const int64_t sidx = st / r_eff;
-      const int r = (int)(st % r_eff);
-      const int64_t s = s_first + sidx * a.n_split;
-      if (!mbar_wait(HFULL(w), ph, abort_flag)) { aborted = true; break; }
-      ph ^= 1u;
-      if (!mbar_wait(GFULL((int)(st & 1)), (uint32_t)((st >> 1) & 1), abort_flag)) { aborted = true; break; }
+    int r = 0, sidx = 0, gstage = 0;
+    uint32_t hph = 0u, gph = 0u;
+    for (int st = 0; st < nsteps; ++st) {
+      if (!mbar_wait(HFULL(hw), hph, abort_flag)) { aborted = true; break; }
+      hph ^= 1u;
+      if (!mbar_wait(GFULL(gstage), gph, abort_flag)) { aborted = true; break; }
       fence_after();
       // T of the previous sample tile: its last T MMAs were committed before this H
-      if (w == 1 && r == 0 && sidx > 0) write_t(s - a.n_split);
+      if (hw == 1 && sub == 0 && r == 0 && sidx > 0) write_t(s_first + (int64_t)(sidx - 1) * a.n_split);
 
       const int64_t jglob = jb + (int64_t)r * TILE + jl;
-      const uint8_t* gs = sm + OFF_G + (int)(st & 1) * G_TILE_BYTES + (jl >> 2) * TILE + w * HALF;
-      uint8_t* ta = sm + OFF_A + (int)(st & 1) * AB_TILE_BYTES;
-      uint8_t* tb = sm + OFF_B + (int)(st & 1) * AB_TILE_BYTES;
+      const uint8_t* gs = sm + OFF_G + gstage * G_TILE_BYTES + (jl >> 2) * G_ROW + colb;
+      uint8_t* ta = sm + OFF_A + (st & 1) * AB_TILE_BYTES;
+      uint8_t* tb = sm + OFF_B + (st & 1) * AB_TILE_BYTES;
       uint32_t hv[2][16], cv[2][16];
       tmem_ld16(trow, hv[0]);
       tmem_ld16(trow + HALF, cv[0]);
       tmem_wait_ld();
 #pragma unroll
-      for (int c = 0; c < HALF / 16; ++c) {
+      for (int c = 0; c < WG_COLS / 16; ++c) {
         const int cur = c & 1;
-        if (c + 1 < HALF / 16) {
+        if (c + 1 < WG_COLS / 16) {
           tmem_ld16(trow + 16 * (c + 1), hv[cur ^ 1]);
           tmem_ld16(trow + HALF + 16 * (c + 1), cv[cur ^ 1]);
         }
-        const int col0 = w * HALF + 16 * c;     // sample column inside the step's tile
+        const int col0 = colb + 16 * c;
         const uint4 gw = *reinterpret_cast<const uint4*>(gs + 16 * c);
         const uint32_t words[4] = {gw.x, gw.y, gw.z, gw.w};
         uint32_t ap[8], bp[8];
@@ -478,17 +533,20 @@ __global__ void __launch_bounds__(TPB, 1) em_sweep_tc_kernel(Args a) {
         *reinterpret_cast<uint4*>(ta + off_ab(jl, col0 + 8)) = make_uint4(ap[4], ap[5], ap[6], ap[7]);
         *reinterpret_cast<uint4*>(tb + off_ab(jl, col0)) = make_uint4(bp[0], bp[1], bp[2], bp[3]);
         *reinterpret_cast<uint4*>(tb + off_ab(jl, col0 + 8)) = make_uint4(bp[4], bp[5], bp[6], bp[7]);
-        tmem_wait_ld();
+        if (c + 1 < WG_COLS / 16) tmem_wait_ld();
       }
       fence_async_smem();
       fence_before();
-      mbar_arrive(ABREADY(w));
+      mbar_arrive(ABREADY(hw));
+      if (++r == r_eff) { r = 0; ++sidx; }
+      if (++gstage == NG) { gstage = 0; gph ^= 1u; }
     }
   }
 
-  // ---- epilogue: wait for the last MMAs (committed to HFULL(1) as completion nhalf/2)
-  if (!aborted && nhalf > 0) {
-    if (!mbar_wait(HFULL(1), (uint32_t)((nhalf >> 1) & 1), abort_flag)) aborted = true;
+  // ---- epilogue: wait for the last MMAs (the last step's commit is completion nsteps of
+  // hfull[1]; the prologue's was completion 0)
+  if (!aborted) {
+    if (!mbar_wait(HFULL(1), (uint32_t)(nsteps & 1), abort_flag)) aborted = true;
   }
   if (__syncthreads_or(aborted)) {
     if (tid == 0) atomicExch(a.err, ADX_ERR_TIMEOUT);
@@ -501,9 +559,10 @@ __global__ void __launch_bounds__(TPB, 1) em_sweep_tc_kernel(Args a) {
     }
   } else {
     fence_after();
-    if (warp >= 4 && warp < 8) write_t(s_first + (n_my - 1) * a.n_split);
+    if (warp >= 4 && warp < 8 && HALF_WGS == 1) write_t(s_first + (int64_t)(n_my - 1) * a.n_split);
+    if (warp >= 8 && warp < 12 && HALF_WGS == 2) write_t(s_first + (int64_t)(n_my - 1) * a.n_split);
     if (warp < 8) {
-      // A/B of every SNP tile: warpgroup 0 reads A, warpgroup 1 reads B
+      // A/B of every SNP tile: warps 0-3 read A, warps 4-7 read B
       const int wg = warp >> 2, wq = warp & 3;
       for (int r = 0; r < r_eff; ++r) {
         uint32_t v[16];
@@ -540,8 +599,10 @@ int tc_plan(int64_t M, int64_t N, int K, int64_t& n_stile, int& n_split, int& n_
   return ADX_OK;
 }
 
+size_t tc_q_bytes(int64_t n_stile) { return (size_t)n_stile * tc::P_TILE_BYTES; }
+
 int tc_sweep(const uint8_t* G, const float* P, const float* Q, int64_t M, int64_t N, int K,
-             int64_t n_stile, int n_split, int n_mblk, float* ABp, float* Tp, int* err,
+             int64_t n_stile, int n_split, int n_mblk, float* ABp, float* Tp, void* Qb, int* err,
              cudaStream_t st) {
   static bool attr_set[64] = {false};
   int dev = 0;
@@ -551,7 +612,10 @@ int tc_sweep(const uint8_t* G, const float* P, const float* Q, int64_t M, int64_
                                       tc::SMEM_ALLOC));
     attr_set[dev] = true;
   }
-  tc::Args a{G, P, Q, M, N, K, n_stile, n_split, n_mblk, ABp, Tp, err};
+  uint8_t* qb = static_cast<uint8_t*>(Qb);
+  tc::q_to_bf16_kernel<<<(unsigned)ceil_div(n_stile * tc::TILE * 2, 256), 256, 0, st>>>(Q, N, K, n_stile, qb);
+  ADX_LAUNCH_CHECK();
+  tc::Args a{G, P, qb, M, N, K, n_stile, n_split, n_mblk, ABp, Tp, err};
   tc::em_sweep_tc_kernel<<<(unsigned)(n_split * n_mblk), tc::TPB, tc::SMEM_ALLOC, st>>>(a);
   ADX_LAUNCH_CHECK();
   return ADX_OK;
