@@ -463,10 +463,22 @@ __global__ void __launch_bounds__(TPB, 1) em_sweep_tc_kernel(Args a) {
       if (!mbar_wait(ABREADY(1), pab1, abort_flag)) { aborted = true; break; }
       pab1 ^= 1u;
       fence_after();
+      // The next half-1 H goes ahead of this step's A/B/T batch in the (in-order) tensor pipe
+      // and is committed first, so the half-1 warpgroups do not wait for the batch. Where
+      // the next step starts a sample tile the commit follows the batch instead: those
+      // warpgroups read T out of tensor memory after it, so it must cover the tile's last
+      // T MMAs. (The batch's a/b buffer is rewritten two steps later, after commits that
+      // cover it; the last step's commit covers everything.)
       if (lane == 0) {
-        issue_abt(r, qb, st & 1, sidx > 0);
-        if (more) issue_h(r1, qb1, 1);
-        mma_commit(HFULL(1));
+        if (more && r1 != 0) {
+          issue_h(r1, qb1, 1);
+          mma_commit(HFULL(1));
+          issue_abt(r, qb, st & 1, sidx > 0);
+        } else {
+          issue_abt(r, qb, st & 1, sidx > 0);
+          if (more) issue_h(r1, qb1, 1);
+          mma_commit(HFULL(1));
+        }
       }
       __syncwarp();
       r = r1; sidx = sidx1; qb = qb1; qpar = qpar1;
