@@ -43,6 +43,14 @@ SIGNATURES: dict[str, list] = {
     "adx_loglik_workspace_bytes": [I64, I64, c_int, c_int, P],
     "adx_loglik": [P, I64, I64, c_int, c_int, P, P, P, P, c_size_t, P],
     "adx_loglik_noalloc": [P, I64, I64, c_int, c_int, P, P, P, P],
+    "adx_rsvd_rows": [P, I64, I64, P, P, c_int, P, P],
+    "adx_rsvd_workspace_bytes": [I64, I64, c_int, P],
+    "adx_rsvd_cols": [P, I64, I64, P, P, c_int, c_int, P, P, c_size_t, P],
+    "adx_bvls": [P, P, I64, c_int, c_double, c_double, P, P],
+    "adx_grad_hess_q": [P, I64, I64, c_int, P, P, P, P, P],
+    "adx_grad_hess_p": [P, I64, I64, c_int, P, P, P, P, P],
+    "adx_sqp_q": [P, P, P, P, I64, c_int, P, P],
+    "adx_sqp_p": [P, P, P, I64, c_int, P, P],
 }
 _RESTYPE = {"adx_version": ctypes.c_char_p, "adx_last_error": ctypes.c_char_p}
 

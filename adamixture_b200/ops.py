@@ -55,8 +55,9 @@ class Workspace:
     _bufs: dict = {}
 
     @classmethod
-    def get(cls, device: torch.device, nbytes: int) -> torch.Tensor:
-        key = (device.type, device.index)
+    def get(cls, device: torch.device, nbytes: int, tag: str = "em") -> torch.Tensor:
+        """Buffers of different tags never alias (the E-step's status word must survive)."""
+        key = (device.type, device.index, tag)
         buf = cls._bufs.get(key)
         if buf is None or buf.numel() < nbytes:
             cls._bufs[key] = None
@@ -255,8 +256,10 @@ _registered = False
 
 
 def register_reference_ops() -> None:
-    """Register ``pack2bit::unpack2bit_gpu_chunk_uint8`` and ``pack2bit::unpack2bit_gpu_chunk_center``
-    (same schemas as the reference) on the CUDA dispatch key, backed by this library."""
+    """Register the reference's extension operators (same schemas) on the CUDA dispatch key,
+    backed by this library: ``pack2bit::unpack2bit_gpu_chunk_uint8``,
+    ``pack2bit::unpack2bit_gpu_chunk_center``, ``bvls_kernel::batch_bvls_bpp_cuda``,
+    ``sqp_kernel::sqp_solve_q_cuda`` and ``sqp_kernel::sqp_solve_p_cuda``."""
     global _registered
     if _registered:
         return
@@ -274,5 +277,111 @@ def register_reference_ops() -> None:
 
     lib.impl("unpack2bit_gpu_chunk_uint8", _u8, "CUDA")
     lib.impl("unpack2bit_gpu_chunk_center", _center, "CUDA")
-    register_reference_ops._lib = lib  # keep the registration alive
+
+    # bvls_kernel.cu:224-230 and sqp_kernel.cu:377-385
+    blib = torch.library.Library("bvls_kernel", "DEF")
+    blib.define("batch_bvls_bpp_cuda(Tensor A, Tensor B, float lower, float upper) -> Tensor")
+    blib.impl("batch_bvls_bpp_cuda",
+              lambda A, B, lower, upper: bvls(A.contiguous(), B.contiguous(), lower, upper), "CUDA")
+    slib = torch.library.Library("sqp_kernel", "DEF")
+    slib.define("sqp_solve_q_cuda(Tensor XtX_q, Tensor Xtz_q, Tensor Q, Tensor v_kk, int N, int K) -> Tensor")
+    slib.define("sqp_solve_p_cuda(Tensor XtX_p, Tensor Xtz_p, Tensor P, int M, int K) -> Tensor")
+    slib.impl("sqp_solve_q_cuda", lambda H, g, Q, v, N, K: sqp_solve_q(
+        H.contiguous(), g.contiguous(), Q.contiguous(), v.contiguous(), N, K), "CUDA")
+    slib.impl("sqp_solve_p_cuda", lambda H, g, P, M, K: sqp_solve_p(
+        H.contiguous(), g.contiguous(), P.contiguous(), M, K), "CUDA")
+    register_reference_ops._lib = (lib, blib, slib)  # keep the registrations alive
     _registered = True
+
+
+# ---------------------------------------------------------------- initialisation
+
+def rsvd_rows(G: torch.Tensor, f: torch.Tensor, B: torch.Tensor, M: int,
+              out: torch.Tensor | None = None) -> torch.Tensor:
+    """``Xc @ B`` for the centred genotypes (float32 ``[M, L]``), B float32 ``[N, L]``."""
+    _check(G, "G", torch.uint8)
+    _check(f, "f", torch.float32, G.device)
+    _check(B, "B", torch.float32, G.device)
+    N, L = B.shape
+    Y = torch.empty((M, L), dtype=torch.float32, device=G.device) if out is None else out
+    _check(Y, "out", torch.float32, G.device)
+    call("adx_rsvd_rows", G.data_ptr(), M, N, f.data_ptr(), B.data_ptr(), L, Y.data_ptr(),
+         _stream(G.device))
+    return Y
+
+
+def rsvd_cols(G: torch.Tensor, f: torch.Tensor, Y: torch.Tensor, M: int,
+              out: torch.Tensor | None = None, accumulate: bool = False) -> torch.Tensor:
+    """``Xc.T @ Y`` (float32 ``[N, L]``; added to ``out`` when ``accumulate``)."""
+    _check(G, "G", torch.uint8)
+    _check(f, "f", torch.float32, G.device)
+    _check(Y, "Y", torch.float32, G.device)
+    N = G.shape[1]
+    L = Y.shape[1]
+    Z = torch.empty((N, L), dtype=torch.float32, device=G.device) if out is None else out
+    _check(Z, "out", torch.float32, G.device)
+    nb = query_size("adx_rsvd_workspace_bytes", M, N, L)
+    ws = Workspace.get(G.device, nb, "rsvd")
+    call("adx_rsvd_cols", G.data_ptr(), M, N, f.data_ptr(), Y.data_ptr(), L, int(bool(accumulate)),
+         Z.data_ptr(), ws.data_ptr(), ws.numel(), _stream(G.device))
+    return Z
+
+
+def bvls(A: torch.Tensor, B: torch.Tensor, lower: float, upper: float) -> torch.Tensor:
+    """Row-batched bounded least squares (float64): ``argmin 1/2 x'Ax - b'x`` in the box."""
+    _check(A, "A", torch.float64)
+    _check(B, "B", torch.float64, A.device)
+    M, K = B.shape
+    if A.shape != (K, K):
+        raise ValueError("A must be K x K")
+    X = torch.empty_like(B)
+    call("adx_bvls", A.data_ptr(), B.data_ptr(), M, K, float(lower), float(upper), X.data_ptr(),
+         _stream(A.device))
+    return X
+
+
+# ---------------------------------------------------------------- original ADMIXTURE (BR-QN)
+
+def grad_hess_q(G: torch.Tensor, P: torch.Tensor, Q: torch.Tensor, M: int, XtX_q=None, Xtz_q=None):
+    _check(G, "G", torch.uint8)
+    _check(P, "P", torch.float64, G.device)
+    _check(Q, "Q", torch.float64, G.device)
+    N, K = Q.shape
+    XtX_q = torch.empty((N, K, K), dtype=torch.float64, device=G.device) if XtX_q is None else XtX_q
+    Xtz_q = torch.empty((N, K), dtype=torch.float64, device=G.device) if Xtz_q is None else Xtz_q
+    call("adx_grad_hess_q", G.data_ptr(), M, N, K, P.data_ptr(), Q.data_ptr(), XtX_q.data_ptr(),
+         Xtz_q.data_ptr(), _stream(G.device))
+    return XtX_q, Xtz_q
+
+
+def grad_hess_p(G: torch.Tensor, P: torch.Tensor, Q: torch.Tensor, M: int, XtX_p=None, Xtz_p=None):
+    _check(G, "G", torch.uint8)
+    _check(P, "P", torch.float64, G.device)
+    _check(Q, "Q", torch.float64, G.device)
+    N, K = Q.shape
+    XtX_p = torch.empty((M, K, K), dtype=torch.float64, device=G.device) if XtX_p is None else XtX_p
+    Xtz_p = torch.empty((M, K), dtype=torch.float64, device=G.device) if Xtz_p is None else Xtz_p
+    call("adx_grad_hess_p", G.data_ptr(), M, N, K, P.data_ptr(), Q.data_ptr(), XtX_p.data_ptr(),
+         Xtz_p.data_ptr(), _stream(G.device))
+    return XtX_p, Xtz_p
+
+
+def sqp_solve_q(XtX_q: torch.Tensor, Xtz_q: torch.Tensor, Q: torch.Tensor, v_kk: torch.Tensor,
+                N: int, K: int) -> torch.Tensor:
+    """Same contract as ``sqp_kernel::sqp_solve_q_cuda`` (Xtz_q already negated)."""
+    for t, nm in ((XtX_q, "XtX_q"), (Xtz_q, "Xtz_q"), (Q, "Q"), (v_kk, "v_kk")):
+        _check(t, nm, torch.float64, Q.device)
+    out = torch.empty((N, K), dtype=torch.float64, device=Q.device)
+    call("adx_sqp_q", XtX_q.data_ptr(), Xtz_q.data_ptr(), Q.data_ptr(), v_kk.data_ptr(), N, K,
+         out.data_ptr(), _stream(Q.device))
+    return out
+
+
+def sqp_solve_p(XtX_p: torch.Tensor, Xtz_p: torch.Tensor, P: torch.Tensor, M: int, K: int) -> torch.Tensor:
+    """Same contract as ``sqp_kernel::sqp_solve_p_cuda`` (Xtz_p already negated)."""
+    for t, nm in ((XtX_p, "XtX_p"), (Xtz_p, "Xtz_p"), (P, "P")):
+        _check(t, nm, torch.float64, P.device)
+    out = torch.empty((M, K), dtype=torch.float64, device=P.device)
+    call("adx_sqp_p", XtX_p.data_ptr(), Xtz_p.data_ptr(), P.data_ptr(), M, K, out.data_ptr(),
+         _stream(P.device))
+    return out

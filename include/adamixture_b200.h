@@ -152,6 +152,47 @@ int adx_loglik(const uint8_t* G, int64_t M, int64_t N, int K, int precision, con
 int adx_loglik_noalloc(const uint8_t* G, int64_t M, int64_t N, int K, int precision,
                        const void* P, const void* Q, double* out, void* stream);
 
+/* ---------------------------------------------------------------- initialisation
+ * Shifted randomized SVD products of the centred genotypes Xc[j][i] = g - 2 f_j (0 where
+ * missing; f float32 [M]), float32. They replace the decode-then-GEMM chunk loops of
+ * SVD_gpu (adamixture/model/svd_gpu.py:80-87, 99-107, 133-139) and the centring unpack op
+ * they call (pack2bit.cu:46-77). L <= 80. */
+/* Y[M][L] = Xc B, B float32 [N][L]. */
+int adx_rsvd_rows(const uint8_t* G, int64_t M, int64_t N, const float* f, const float* B, int L,
+                  float* Y, void* stream);
+int adx_rsvd_workspace_bytes(int64_t M, int64_t N, int L, size_t* bytes);
+/* Z[N][L] = Xc' Y (accumulate != 0: Z += Xc' Y), Y float32 [M][L]; partial sums in the
+ * workspace are added in a fixed order. */
+int adx_rsvd_cols(const uint8_t* G, int64_t M, int64_t N, const float* f, const float* Y, int L,
+                  int accumulate, float* Z, void* workspace, size_t workspace_bytes,
+                  void* stream);
+
+/* Batched bounded least squares, float64, one warp per row: X[m] = argmin over
+ * lower <= x <= upper of 1/2 x'Ax - B[m]'x by block principal pivoting, A [K][K] shared.
+ * Replaces bvls_kernel::batch_bvls_bpp_cuda (adamixture/src/utils_c/cuda/bvls_kernel.cu:
+ * 75-164, 188-218), which ALS_gpu (adamixture/model/als_gpu.py:105,115) calls. */
+int adx_bvls(const double* A, const double* B, int64_t M, int K, double lower, double upper,
+             double* X, void* stream);
+
+/* ---------------------------------------------------------------- original ADMIXTURE (BR-QN)
+ * Gradient and Hessian passes over the packed genotypes, float64 (outputs overwritten):
+ * Q side XtX_q [N][K][K], Xtz_q [N][K] (compute_grad_hess_Q_gpu, br_qn_gpu.py:145-179);
+ * P side XtX_p [M][K][K], Xtz_p [M][K] (compute_grad_hess_P_gpu, br_qn_gpu.py:182-214).
+ * Xtz is the gradient as computed there (not yet negated). */
+int adx_grad_hess_q(const uint8_t* G, int64_t M, int64_t N, int K, const double* P,
+                    const double* Q, double* XtX_q, double* Xtz_q, void* stream);
+int adx_grad_hess_p(const uint8_t* G, int64_t M, int64_t N, int K, const double* P,
+                    const double* Q, double* XtX_p, double* Xtz_p, void* stream);
+/* SQP steps, float64, one warp per row; Xtz as the reference's caller passes it (negated,
+ * br_qn_gpu.py:295). Q rows: simplex QP with shift from v_kk [K][K], then projection onto
+ * {q >= 1e-5, sum q = 1} (sqp_kernel::sqp_solve_q_cuda, sqp_kernel.cu:262-286, 320-345).
+ * P rows: box QP, then clamping to [1e-5, 1-1e-5] (sqp_solve_p_cuda, sqp_kernel.cu:
+ * 288-311, 347-370). */
+int adx_sqp_q(const double* XtX_q, const double* Xtz_q, const double* Q, const double* v_kk,
+              int64_t N, int K, double* Q_next, void* stream);
+int adx_sqp_p(const double* XtX_p, const double* Xtz_p, const double* P, int64_t M, int K,
+              double* P_next, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

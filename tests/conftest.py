@@ -44,3 +44,13 @@ def cuda():
     if not torch.cuda.is_available():
         pytest.skip("no CUDA device")
     return torch.device("cuda:0")
+
+
+@pytest.fixture(scope="session")
+def solvers_golden():
+    return _load("solvers")
+
+
+@pytest.fixture(scope="session")
+def demo_gpu():
+    return _load("demo_gpu")

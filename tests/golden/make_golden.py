@@ -3,7 +3,7 @@
 Run from the repository root, in a tree that has the reference sources and the
 compiled reference modules (``make -C oracle``):
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py [edge synth demo demo_gpu solvers]
 
 What it records (all from the reference's own code, imported from its source tree;
 its ``torch.compile`` wrappers run eagerly as float64 torch code on the CPU, with the
@@ -20,6 +20,10 @@ CUDA unpack op replaced by a bit-shift unpacker of the same packed layout):
   same records (trace of 10 iterations).
 * ``edge.npz``: a tiny cohort (N=37, M=29, K=4) with an all-missing sample and an
   all-missing SNP, with one E-step and the log-likelihood.
+* ``demo_gpu.npz``: the reference's GPU golden files of the demo run (SVD, ALS, BR-QN and
+  Adam-EM results).
+* ``solvers.npz``: the reference's CPU BVLS (K = 1..64), gradient/Hessian and SQP
+  outputs on seeded problems.
 """
 from __future__ import annotations
 
@@ -160,8 +164,72 @@ def edge(em, utils):
     print("edge.npz", rec["loglik0"])
 
 
+def demo_gpu():
+    """The reference's GPU golden files for the demo run (K=7, seed 42, power 5, tol_svd
+    0.1): randomized SVD, ALS init (shared by both optimisers), converged BR-QN and
+    Adam-EM P/Q (adamixture/demo/outputs/gpu/*, checked by tests/test_cuda.py there)."""
+    out = refmods.REFERENCE_TREE / "adamixture" / "demo" / "outputs" / "gpu"
+    rec = {}
+    for nm in ("svd.U", "svd.S", "svd.V", "als.P", "als.Q"):
+        rec[nm.replace(".", "_")] = np.loadtxt(out / "adamem" / f"demo_run.{nm}.expected")
+    for alg in ("adamem", "brqn"):
+        for nm in ("P", "Q"):
+            rec[f"{alg}_{nm}"] = np.loadtxt(out / alg / f"demo_run.{alg}.{nm}.expected")
+    np.savez_compressed(OUT / "demo_gpu.npz", **rec)
+    print("demo_gpu.npz", {k: v.shape for k, v in rec.items()})
+
+
+def solvers():
+    """Inputs and outputs of the reference's CPU BVLS, gradient/Hessian and SQP kernels
+    (the compiled bvls.pyx / sqp.pyx) on seeded problems."""
+    from adamixture_b200.src.simulate import make_cohort
+
+    bv = refmods.load("bvls")
+    sq = refmods.load("sqp")
+    rec = {}
+    rng = np.random.default_rng(21)
+    for K in (1, 3, 7, 12, 20, 40, 64):
+        X = rng.normal(size=(3 * K + 5, K))
+        A = X.T @ X + 0.1 * np.eye(K)
+        xt = rng.uniform(-0.6, 1.6, size=(96, K))
+        B = xt @ A + rng.normal(0, 0.05, size=(96, K))
+        out = np.zeros_like(B)
+        bv.batch_bvls_bpp(A, np.ascontiguousarray(B), out, 0.0, 1.0)
+        rec[f"bvls{K}_A"], rec[f"bvls{K}_B"], rec[f"bvls{K}_X"] = A, B, out
+    _, _, vt = torch.linalg.svd(torch.ones((1, 1), dtype=torch.float64), full_matrices=True)
+    for tag, (N, M, K, seed) in {"a": (61, 150, 5, 5), "b": (40, 90, 12, 6), "c": (33, 70, 2, 8)}.items():
+        coh = make_cohort(N, M, K, F=0.1, alpha=0.5, miss=0.05, seed=seed)
+        G = np.ascontiguousarray(coh.genotypes())
+        r2 = np.random.default_rng(seed)
+        P = np.clip(coh.P + r2.normal(0, 0.1, coh.P.shape), 1e-5, 1 - 1e-5)
+        Q = np.clip(coh.Q + r2.uniform(0, 0.3, coh.Q.shape), 1e-5, 1 - 1e-5)
+        Q /= Q.sum(1, keepdims=True)
+        _, _, vt = torch.linalg.svd(torch.ones((1, K), dtype=torch.float64), full_matrices=True)
+        v_kk = np.ascontiguousarray(vt.t().numpy())
+        XtX_q = np.zeros((N, K, K)); Xtz_q = np.zeros((N, K))
+        XtX_p = np.zeros((M, K, K)); Xtz_p = np.zeros((M, K))
+        Q_next = np.zeros((N, K)); P_next = np.zeros((M, K))
+        sq.update_q_sqp(G, Q, Q_next, P, XtX_q, Xtz_q, v_kk, M, N, K)
+        sq.update_p_sqp(G, Q, P, P_next, XtX_p, Xtz_p, M, N, K)
+        rec.update({f"{tag}_packed": coh.packed(), f"{tag}_G": G, f"{tag}_P": P, f"{tag}_Q": Q,
+                    f"{tag}_v_kk": v_kk, f"{tag}_XtX_q": XtX_q, f"{tag}_Xtz_q": Xtz_q,
+                    f"{tag}_XtX_p": XtX_p, f"{tag}_Xtz_p": Xtz_p, f"{tag}_Q_next": Q_next,
+                    f"{tag}_P_next": P_next})
+    np.savez_compressed(OUT / "solvers.npz", **rec)
+    print("solvers.npz", len(rec))
+
+
 if __name__ == "__main__":
-    em, utils = reference()
-    edge(em, utils)
-    synth(em, utils)
-    demo(em, utils)
+    which = set(sys.argv[1:]) or {"edge", "synth", "demo", "demo_gpu", "solvers"}
+    if which & {"edge", "synth", "demo"}:
+        em, utils = reference()
+        if "edge" in which:
+            edge(em, utils)
+        if "synth" in which:
+            synth(em, utils)
+        if "demo" in which:
+            demo(em, utils)
+    if "demo_gpu" in which:
+        demo_gpu()
+    if "solvers" in which:
+        solvers()
