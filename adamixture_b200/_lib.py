@@ -51,6 +51,13 @@ SIGNATURES: dict[str, list] = {
     "adx_grad_hess_p": [P, I64, I64, c_int, P, P, P, P, P],
     "adx_sqp_q": [P, P, P, P, I64, c_int, P, P],
     "adx_sqp_p": [P, P, P, I64, c_int, P, P],
+    "adx_project_simplex": [P, I64, c_int, P],
+    "adx_project_box": [P, I64, c_int, P],
+    "adx_cv_workspace_bytes": [P],
+    "adx_cv_mask_list": [P, c_size_t, I64, I64, P, I64, P, c_size_t, P],
+    "adx_cv_mask_hash": [P, c_size_t, P, I64, I64, c_uint64, c_int, c_int, P],
+    "adx_cv_deviance_list": [P, I64, I64, c_int, P, P, P, I64, P, P, c_size_t, P],
+    "adx_cv_deviance_hash": [P, I64, I64, c_int, P, P, c_uint64, c_int, c_int, P, P, c_size_t, P],
 }
 _RESTYPE = {"adx_version": ctypes.c_char_p, "adx_last_error": ctypes.c_char_p}
 

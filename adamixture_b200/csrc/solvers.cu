@@ -467,3 +467,50 @@ extern "C" int adx_sqp_p(const double* XtX, const double* Xtz, const double* P, 
   if (M == 0) return ADX_OK;
   return launch_sqp<false>(XtX, Xtz, P, nullptr, M, K, P_next, stream);
 }
+
+// ---------------------------------------------------------------- projections
+
+namespace adx {
+namespace solve {
+
+// Thread per row: Q rows onto {q >= 1e-5, sum q = 1} (sqp.pyx:112-146), P rows clamped to
+// [1e-5, 1 - 1e-5] (sqp.pyx:148-151).
+__global__ void project_simplex_kernel(double* __restrict__ X, int64_t rows, int K) {
+  const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= rows) return;
+  double b[ADX_MAX_K];
+  for (int k = 0; k < K; ++k) b[k] = X[r * K + k];
+  project_simplex_row(b, K, 1e-5);
+  for (int k = 0; k < K; ++k) X[r * K + k] = b[k];
+}
+
+__global__ void project_box_kernel(double* __restrict__ X, int64_t n) {
+  const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e < n) X[e] = fmin(fmax(X[e], 1e-5), 1.0 - 1e-5);
+}
+
+}  // namespace solve
+}  // namespace adx
+
+extern "C" int adx_project_simplex(double* Q, int64_t N, int K, void* stream) {
+  if (!Q || N < 0 || K < 1 || K > ADX_MAX_K) {
+    adx_set_message("adx_project_simplex: bad argument");
+    return ADX_ERR_ARG;
+  }
+  if (N == 0) return ADX_OK;
+  solve::project_simplex_kernel<<<(unsigned)ceil_div(N, 128), 128, 0, as_stream(stream)>>>(Q, N, K);
+  ADX_LAUNCH_CHECK();
+  return ADX_OK;
+}
+
+extern "C" int adx_project_box(double* P, int64_t M, int K, void* stream) {
+  if (!P || M < 0 || K < 1 || K > ADX_MAX_K) {
+    adx_set_message("adx_project_box: bad argument");
+    return ADX_ERR_ARG;
+  }
+  const int64_t n = M * K;
+  if (n == 0) return ADX_OK;
+  solve::project_box_kernel<<<(unsigned)ceil_div(n, 256), 256, 0, as_stream(stream)>>>(P, n);
+  ADX_LAUNCH_CHECK();
+  return ADX_OK;
+}

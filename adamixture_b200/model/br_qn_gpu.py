@@ -47,7 +47,11 @@ def _v_kk(K: int, device) -> torch.Tensor:
     return vt.t().to(device=device, dtype=torch.float64).contiguous()
 
 
-def _optimize_original_gpu_once(G, P, Q, max_iter, K, M, N, tol, Q_hist, patience, device):
+def _optimize_original_gpu_once(G, P, Q, max_iter, K, M, N, tol, Q_hist, patience, device,
+                                qn_projection="clamp", verbose=True):
+    """``qn_projection``: how the extrapolated point returns to the feasible set -- "clamp"
+    (clamp and renormalise, the GPU reference, br_qn_gpu.py:341) or "simplex" (box for P,
+    simplex projection for Q, the CPU reference, adamixture/model/br_qn.py:157-158)."""
     dt = torch.float64
     v_kk = _v_kk(K, device)
     XtX_q = torch.zeros((N, K, K), dtype=dt, device=device)
@@ -113,7 +117,11 @@ def _optimize_original_gpu_once(G, P, Q, max_iter, K, M, N, tol, Q_hist, patienc
         torch.sub(x1, x_qn, out=x_qn)
         P_qn.copy_(x_qn[:mk].view(M, K))
         Q_qn.copy_(x_qn[mk:].view(-1, K))
-        _mapPQ_gpu(P_qn, Q_qn)
+        if qn_projection == "simplex":
+            ops.project_box_(P_qn)
+            ops.project_simplex_(Q_qn)
+        else:
+            _mapPQ_gpu(P_qn, Q_qn)
 
         ll_qn = logl(P_qn, Q_qn)
         if ll_qn > ll_prev:
@@ -134,15 +142,19 @@ def _optimize_original_gpu_once(G, P, Q, max_iter, K, M, N, tol, Q_hist, patienc
             wait += 1
         else:
             wait = 0
-        log.info(f"    Iteration {it}, Log-likelihood: {ll_new:.1f}, Time: {time.time() - t_it:.3f}s")
+        if verbose:
+            log.info(f"    Iteration {it}, Log-likelihood: {ll_new:.1f}, Time: {time.time() - t_it:.3f}s")
         if abs(ll_new - ll_prev) < tol:
-            log.info(f"    Converged at iteration {it}.")
+            if verbose:
+                log.info(f"    Converged at iteration {it}.")
             break
         if wait >= patience:
-            log.info(f"    Converged at iteration {it} after {wait} iterations without improvement.")
+            if verbose:
+                log.info(f"    Converged at iteration {it} after {wait} iterations without improvement.")
             break
         ll_prev = ll_new
-    log.info(f"\n    Final log-likelihood: {ll_best:.1f}")
+    if verbose:
+        log.info(f"\n    Final log-likelihood: {ll_best:.1f}")
     return P_best, Q_best
 
 
@@ -156,3 +168,14 @@ def optimize_original_gpu(G: torch.Tensor, P: torch.Tensor, Q: torch.Tensor, max
     P_w = P.to(device=G.device, dtype=torch.float64).clone().contiguous()
     Q_w = Q.to(device=G.device, dtype=torch.float64).clone().contiguous()
     return _optimize_original_gpu_once(G, P_w, Q_w, max_iter, K, M, N, tol, Q_hist, patience, G.device)
+
+
+def polish_sqp_qn(G: torch.Tensor, P_init, Q_init, M: int, N: int, K: int,
+                  n_iters: int = 3, Q_hist: int = 3) -> tuple[torch.Tensor, torch.Tensor]:
+    """Exactly ``n_iters`` SQP + ZAL iterations from a warm start with early stopping off
+    (tol 0, patience n_iters + 1) and the CPU reference's simplex projection of the
+    extrapolated point: adamixture/model/br_qn.py:50-70, on the GPU."""
+    P = torch.as_tensor(P_init, dtype=torch.float64).to(G.device).clone().contiguous()
+    Q = torch.as_tensor(Q_init, dtype=torch.float64).to(G.device).clone().contiguous()
+    return _optimize_original_gpu_once(G, P, Q, n_iters, K, M, N, 0.0, Q_hist, n_iters + 1, G.device,
+                                       qn_projection="simplex", verbose=False)

@@ -385,3 +385,65 @@ def sqp_solve_p(XtX_p: torch.Tensor, Xtz_p: torch.Tensor, P: torch.Tensor, M: in
     call("adx_sqp_p", XtX_p.data_ptr(), Xtz_p.data_ptr(), P.data_ptr(), M, K, out.data_ptr(),
          _stream(P.device))
     return out
+
+
+def project_simplex_(Q: torch.Tensor) -> torch.Tensor:
+    """Project float64 Q rows onto {q >= 1e-5, sum q = 1} in place."""
+    _check(Q, "Q", torch.float64)
+    call("adx_project_simplex", Q.data_ptr(), Q.shape[0], Q.shape[1], _stream(Q.device))
+    return Q
+
+
+def project_box_(P: torch.Tensor) -> torch.Tensor:
+    """Clamp float64 P into [1e-5, 1 - 1e-5] in place."""
+    _check(P, "P", torch.float64)
+    call("adx_project_box", P.data_ptr(), P.shape[0], P.shape[1], _stream(P.device))
+    return P
+
+
+# ---------------------------------------------------------------- cross-validation
+
+def masked_copy(G: torch.Tensor) -> torch.Tensor:
+    """A copy of packed G in a buffer padded to whole 32-bit words (the masking kernels
+    hide entries with 32-bit atomics); returns the [rows, N] view."""
+    _check(G, "G", torch.uint8)
+    n = G.numel()
+    buf = torch.empty(((n + 3) // 4) * 4, dtype=torch.uint8, device=G.device)
+    view = buf[:n].view(G.shape)
+    view.copy_(G)
+    return view
+
+
+def _padded_bytes(Gm: torch.Tensor) -> int:
+    return Gm.untyped_storage().nbytes() - Gm.storage_offset()
+
+
+def cv_mask_list(Gm: torch.Tensor, M: int, idx: torch.Tensor) -> None:
+    """Hide the entries at flat indices ``idx`` (int64, j*N + i) in the masked copy ``Gm``."""
+    _check(idx, "idx", torch.int64, Gm.device)
+    ws = Workspace.get(Gm.device, query_size("adx_cv_workspace_bytes"), "cv")
+    call("adx_cv_mask_list", Gm.data_ptr(), _padded_bytes(Gm) // 4 * 4, M, Gm.shape[1], idx.data_ptr(),
+         idx.numel(), ws.data_ptr(), ws.numel(), _stream(Gm.device))
+
+
+def cv_mask_hash(Gm: torch.Tensor, G0: torch.Tensor, M: int, seed: int, n_folds: int, fold: int) -> None:
+    """Hide fold ``fold`` of the hash rule (observed entries of ``G0``) in ``Gm``."""
+    call("adx_cv_mask_hash", Gm.data_ptr(), _padded_bytes(Gm) // 4 * 4, G0.data_ptr(), M, G0.shape[1],
+         int(seed) & 0xFFFFFFFFFFFFFFFF, n_folds, fold, _stream(Gm.device))
+
+
+def cv_deviance_list(G0, P, Q, M, idx) -> float:
+    ws = Workspace.get(G0.device, query_size("adx_cv_workspace_bytes"), "cv")
+    out = torch.empty(1, dtype=torch.float64, device=G0.device)
+    call("adx_cv_deviance_list", G0.data_ptr(), M, G0.shape[1], Q.shape[1], P.data_ptr(), Q.data_ptr(),
+         idx.data_ptr(), idx.numel(), out.data_ptr(), ws.data_ptr(), ws.numel(), _stream(G0.device))
+    return float(out.item())
+
+
+def cv_deviance_hash(G0, P, Q, M, seed, n_folds, fold) -> float:
+    ws = Workspace.get(G0.device, query_size("adx_cv_workspace_bytes"), "cv")
+    out = torch.empty(1, dtype=torch.float64, device=G0.device)
+    call("adx_cv_deviance_hash", G0.data_ptr(), M, G0.shape[1], Q.shape[1], P.data_ptr(), Q.data_ptr(),
+         int(seed) & 0xFFFFFFFFFFFFFFFF, n_folds, fold, out.data_ptr(), ws.data_ptr(), ws.numel(),
+         _stream(G0.device))
+    return float(out.item())

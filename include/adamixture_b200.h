@@ -193,6 +193,31 @@ int adx_sqp_q(const double* XtX_q, const double* Xtz_q, const double* Q, const d
 int adx_sqp_p(const double* XtX_p, const double* Xtz_p, const double* P, int64_t M, int K,
               double* P_next, void* stream);
 
+/* Projections of rows onto the feasible sets, float64, in place: Q rows onto
+ * {q >= 1e-5, sum q = 1} (project_q_simplex, adamixture/src/utils_c/cython/sqp.pyx:112-146,
+ * 330-333), P entries clamped to [1e-5, 1 - 1e-5] (project_p_box, sqp.pyx:148-151, 335-338). */
+int adx_project_simplex(double* Q, int64_t N, int K, void* stream);
+int adx_project_box(double* P, int64_t M, int K, void* stream);
+
+/* ---------------------------------------------------------------- cross-validation
+ * Held-out entries of a fold are hidden (set to 3) in a copy G of the packed matrix; the
+ * copy must be 4-byte aligned and g_bytes (its allocation) a multiple of 4 covering it.
+ * Folds as a list of flat indices j*N + i (int64; the reference's shuffled-list rule,
+ * adamixture/src/cv.py:202-222, mask_entries_i32/i64 in br_qn.pyx) or by the reference's
+ * hash of the flat index (cv.py:58-78, 117-147). The deviance sums (deviance_squared_sum,
+ * br_qn.pyx:92-150) read the unmasked G0 and write a device double. */
+int adx_cv_workspace_bytes(size_t* bytes);
+int adx_cv_mask_list(uint8_t* G, size_t g_bytes, int64_t M, int64_t N, const int64_t* idx,
+                     int64_t n, void* workspace, size_t workspace_bytes, void* stream);
+int adx_cv_mask_hash(uint8_t* G, size_t g_bytes, const uint8_t* G0, int64_t M, int64_t N,
+                     uint64_t seed, int n_folds, int fold, void* stream);
+int adx_cv_deviance_list(const uint8_t* G0, int64_t M, int64_t N, int K, const double* P,
+                         const double* Q, const int64_t* idx, int64_t n, double* out,
+                         void* workspace, size_t workspace_bytes, void* stream);
+int adx_cv_deviance_hash(const uint8_t* G0, int64_t M, int64_t N, int K, const double* P,
+                         const double* Q, uint64_t seed, int n_folds, int fold, double* out,
+                         void* workspace, size_t workspace_bytes, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -263,3 +263,21 @@ def rsvd_rows(G, f, B):
 
 def rsvd_cols(G, f, Y):
     return centred(G, f).T @ np.asarray(Y, dtype=np.float64)
+
+
+# ---------------------------------------------------------------- cross-validation score
+
+def deviance_sum(G, P, Q, flat):
+    """Sum of g log(g/mu) + (2-g) log((2-g)/(2-mu)) over the entries at flat indices j*N+i,
+    mu = clamp(2 P_j.Q_i, 1e-10, 2-1e-10) (adamixture/src/utils_c/cython/br_qn.pyx:92-150)."""
+    N = G.shape[1]
+    j, i = np.divmod(np.asarray(flat, dtype=np.int64), N)
+    g = G[j, i].astype(np.float64)
+    keep = g != 3
+    j, i, g = j[keep], i[keep], g[keep]
+    mu = np.clip(2.0 * np.einsum("ek,ek->e", Q[i], P[j]), 1e-10, 2.0 - 1e-10)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        ta = np.where(g > 0, g * np.log(np.where(g > 0, g, 1.0) / mu), 0.0)
+        rem = 2.0 - g
+        tb = np.where(rem > 0, rem * np.log(np.where(rem > 0, rem, 1.0) / (2.0 - mu)), 0.0)
+    return float((ta + tb).sum())

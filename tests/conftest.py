@@ -54,3 +54,8 @@ def solvers_golden():
 @pytest.fixture(scope="session")
 def demo_gpu():
     return _load("demo_gpu")
+
+
+@pytest.fixture(scope="session")
+def cv_proj():
+    return _load("cv_proj")

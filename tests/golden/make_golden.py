@@ -3,7 +3,7 @@
 Run from the repository root, in a tree that has the reference sources and the
 compiled reference modules (``make -C oracle``):
 
-    python tests/golden/make_golden.py [edge synth demo demo_gpu solvers]
+    python tests/golden/make_golden.py [edge synth demo demo_gpu solvers cv_proj]
 
 What it records (all from the reference's own code, imported from its source tree;
 its ``torch.compile`` wrappers run eagerly as float64 torch code on the CPU, with the
@@ -24,6 +24,8 @@ CUDA unpack op replaced by a bit-shift unpacker of the same packed layout):
   Adam-EM results).
 * ``solvers.npz``: the reference's CPU BVLS (K = 1..64), gradient/Hessian and SQP
   outputs on seeded problems.
+* ``cv_proj.npz``: the reference's cross-validation index (5 folds, seed 42) and fold
+  rules, and its Adam-EM and SQP + ZAL projections, on a seeded cohort (N=90, M=700, K=3).
 """
 from __future__ import annotations
 
@@ -219,9 +221,47 @@ def solvers():
     print("solvers.npz", len(rec))
 
 
+def cv_proj(em, utils):
+    """The reference's CPU cross-validation (cv.py run_cross_validation: shuffled-list folds,
+    5 BR-QN polish iterations, deviance score) and its hash fold rule, plus its GPU-path
+    Adam-EM projection run on the CPU and its CPU SQP + ZAL projection, on a seeded cohort."""
+    from argparse import Namespace
+
+    from adamixture.src import cv, projection
+    from adamixture_b200.src.simulate import make_cohort
+
+    projection.utils.get_unpacker = utils.get_unpacker
+    N, M, K = 90, 700, 3
+    coh = make_cohort(N, M, K, F=0.1, alpha=0.5, miss=0.02, seed=31)
+    G = np.ascontiguousarray(coh.genotypes())
+    P = np.clip(coh.P, 1e-5, 1 - 1e-5)
+    Q = np.clip(coh.Q, 1e-5, 1 - 1e-5)
+    Q /= Q.sum(1, keepdims=True)
+    rec = dict(packed=coh.packed(), G=G, P=P, Q=Q)
+    flat = np.flatnonzero(G != 3).astype(np.int32)
+    rec["cv_shuffled"] = cv._shuffle_non_missing(flat, 42)
+    rec["cv_index"] = np.float64(cv.run_cross_validation(Namespace(cv=5, seed=42), G.copy(), N, M, K, P, Q))
+    probe = (np.arange(20000, dtype=np.int64) * 104729 + 17) % (1 << 40)
+    rec["hash_probe"] = probe
+    rec["hash_fold"] = np.stack([cv._hash_fold_mask(probe, 42, 5, f) for f in range(5)]).argmax(0).astype(np.uint8)
+    rng = np.random.default_rng(42)
+    Q0 = rng.random(size=(N, K))
+    Q0 /= Q0.sum(1, keepdims=True)
+    rec["proj_Q0"] = Q0
+    dev = torch.device("cpu")
+    Qa = projection.optimize_projection_gpu(
+        torch.from_numpy(coh.packed()), torch.from_numpy(P.copy()), torch.from_numpy(Q0.copy()),
+        HP["lr"], HP["beta1"], HP["beta2"], HP["reg_adam"], 10000, HP["check"], M, HP["lr_decay"],
+        HP["min_lr"], HP["patience"], HP["tol"], dev, 8192, 1)
+    rec["proj_adamem_Q"] = Qa.numpy().copy()
+    rec["proj_brqn_Q"] = projection.optimize_projection_original(G, P.copy(), Q0.copy(), 10000, K, M, N, 0.1, 3, 3)
+    np.savez_compressed(OUT / "cv_proj.npz", **rec)
+    print("cv_proj.npz cv_index", rec["cv_index"])
+
+
 if __name__ == "__main__":
-    which = set(sys.argv[1:]) or {"edge", "synth", "demo", "demo_gpu", "solvers"}
-    if which & {"edge", "synth", "demo"}:
+    which = set(sys.argv[1:]) or {"edge", "synth", "demo", "demo_gpu", "solvers", "cv_proj"}
+    if which & {"edge", "synth", "demo", "cv_proj"}:
         em, utils = reference()
         if "edge" in which:
             edge(em, utils)
@@ -229,6 +269,8 @@ if __name__ == "__main__":
             synth(em, utils)
         if "demo" in which:
             demo(em, utils)
+        if "cv_proj" in which:
+            cv_proj(em, utils)
     if "demo_gpu" in which:
         demo_gpu()
     if "solvers" in which:

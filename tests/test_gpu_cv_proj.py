@@ -1,0 +1,110 @@
+"""GPU cross-validation and projection against the reference (tests/golden/cv_proj.npz):
+
+* fold hiding (list and hash rules) bit-exact against numpy on the unpacked matrix;
+* deviance sums against the float64 oracle, relative 1e-12;
+* the CV index of the reference's CPU cross-validation (5 folds, seed 42, shuffled-list
+  rule, 5 BR-QN polish iterations), relative 1e-6;
+* the Adam-EM projection against the reference's float64 path, 1e-5 absolute; the SQP + ZAL
+  projection against the reference's CPU run (which returns the extrapolated point to the
+  simplex by projection where the GPU path clamps and renormalises), 1e-4 absolute, and its
+  log-likelihood within 1e-6 relative.
+"""
+from argparse import Namespace
+
+import numpy as np
+import pytest
+import torch
+
+from oracle import em_oracle as orc
+from oracle import solvers as osv
+
+pytestmark = pytest.mark.gpu
+
+
+def dev(x):
+    return torch.from_numpy(np.ascontiguousarray(x)).cuda()
+
+
+@pytest.fixture(scope="module")
+def ops(cuda):
+    from adamixture_b200 import ops as _ops
+
+    return _ops
+
+
+def test_mask_list_and_hash(ops, cv_proj):
+    from adamixture_b200.src import cv
+
+    G = cv_proj["G"]
+    M, N = G.shape
+    Gd = dev(cv_proj["packed"])
+    flat = cv_proj["cv_shuffled"][2::5].astype(np.int64)
+    Gm = ops.masked_copy(Gd)
+    ops.cv_mask_list(Gm, M, dev(flat))
+    want = G.copy().reshape(-1)
+    want[flat] = 3
+    np.testing.assert_array_equal(Gm.cpu().numpy(), orc.pack(want.reshape(M, N)))
+    Gh = ops.masked_copy(Gd)
+    ops.cv_mask_hash(Gh, Gd, M, 42, 5, 3)
+    allf = np.arange(M * N)
+    hide = cv.hash_fold_mask(allf, 42, 5, 3) & (G.reshape(-1) != 3)
+    want = G.copy().reshape(-1)
+    want[hide] = 3
+    np.testing.assert_array_equal(Gh.cpu().numpy(), orc.pack(want.reshape(M, N)))
+    # deviance sums over the same entries
+    P, Q = dev(cv_proj["P"]), dev(cv_proj["Q"])
+    d_list = ops.cv_deviance_list(Gd, P, Q, M, dev(flat))
+    assert abs(d_list - osv.deviance_sum(G, cv_proj["P"], cv_proj["Q"], flat)) <= 1e-12 * abs(d_list)
+    d_hash = ops.cv_deviance_hash(Gd, P, Q, M, 42, 5, 3)
+    assert abs(d_hash - osv.deviance_sum(G, cv_proj["P"], cv_proj["Q"], allf[hide])) <= 1e-12 * abs(d_hash)
+
+
+def test_cv_index_matches_reference(cuda, cv_proj):
+    from adamixture_b200.src.cv import run_cross_validation
+
+    G = cv_proj["G"]
+    M, N = G.shape
+    K = cv_proj["P"].shape[1]
+    cvi = run_cross_validation(Namespace(cv=5, seed=42), dev(cv_proj["packed"]), N, M, K,
+                               cv_proj["P"], cv_proj["Q"])
+    ref = float(cv_proj["cv_index"])
+    print("cv index", cvi, "reference", ref)
+    assert abs(cvi - ref) <= 1e-6 * abs(ref)
+
+
+def test_cv_hash_rule_runs(cuda, cv_proj):
+    from adamixture_b200.src.cv import run_cross_validation
+
+    G = cv_proj["G"]
+    M, N = G.shape
+    cvi = run_cross_validation(Namespace(cv=5, seed=42), dev(cv_proj["packed"]), N, M, 3,
+                               cv_proj["P"], cv_proj["Q"], fold_rule="hash")
+    assert np.isfinite(cvi) and 0.0 < cvi < 2.0
+    # same order of magnitude as the list rule's index on the same fit
+    assert abs(cvi - float(cv_proj["cv_index"])) < 0.2 * float(cv_proj["cv_index"])
+
+
+def test_projection_adamem_matches_reference(cuda, cv_proj):
+    from adamixture_b200.src.projection import optimize_projection_gpu
+
+    G = dev(cv_proj["packed"])
+    M = cv_proj["G"].shape[0]
+    Q = optimize_projection_gpu(G, dev(cv_proj["P"]), dev(cv_proj["proj_Q0"]), 0.005, 0.80, 0.88, 1e-8,
+                                10000, 5, M, 0.5, 1e-4, 3, 0.1, G.device, 8192, 256)
+    np.testing.assert_allclose(Q.cpu().numpy(), cv_proj["proj_adamem_Q"], atol=1e-5)
+
+
+def test_projection_brqn_matches_reference(cuda, cv_proj):
+    from adamixture_b200.src.projection import optimize_projection_original_gpu
+
+    Gu = cv_proj["G"]
+    M, N = Gu.shape
+    K = cv_proj["P"].shape[1]
+    G = dev(cv_proj["packed"])
+    Q = optimize_projection_original_gpu(G, dev(cv_proj["P"]), dev(cv_proj["proj_Q0"]), 10000, K, M, N,
+                                         0.1, 3, 3, G.device, 8192, 256).cpu().numpy()
+    Qr = cv_proj["proj_brqn_Q"]
+    np.testing.assert_allclose(Q, Qr, atol=1e-4)
+    L, Lr = orc.loglik(Gu, cv_proj["P"], Q), orc.loglik(Gu, cv_proj["P"], Qr)
+    print("brqn projection loglik", L, "reference", Lr, "max |dQ|", np.abs(Q - Qr).max())
+    assert abs(L - Lr) <= 1e-6 * abs(Lr)
