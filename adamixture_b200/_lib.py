@@ -58,6 +58,7 @@ SIGNATURES: dict[str, list] = {
     "adx_cv_mask_hash": [P, c_size_t, P, I64, I64, c_uint64, c_int, c_int, P],
     "adx_cv_deviance_list": [P, I64, I64, c_int, P, P, P, I64, P, P, c_size_t, P],
     "adx_cv_deviance_hash": [P, I64, I64, c_int, P, P, c_uint64, c_int, c_int, P, P, c_size_t, P],
+    "adx_write_text_matrix": [ctypes.c_char_p, P, I64, I64, c_int],
 }
 _RESTYPE = {"adx_version": ctypes.c_char_p, "adx_last_error": ctypes.c_char_p}
 

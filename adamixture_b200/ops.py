@@ -56,7 +56,9 @@ class Workspace:
 
     @classmethod
     def get(cls, device: torch.device, nbytes: int, tag: str = "em") -> torch.Tensor:
-        """Buffers of different tags never alias (the E-step's status word must survive)."""
+        """Buffers of different tags never alias. The "em" buffer belongs to the E-step
+        alone: its first word is the sweep's sticky status, which other scratch users
+        would overwrite."""
         key = (device.type, device.index, tag)
         buf = cls._bufs.get(key)
         if buf is None or buf.numel() < nbytes:
@@ -121,7 +123,7 @@ def bed_to_packed(bed_rows: torch.Tensor, N: int, M: int) -> torch.Tensor:
     dev = bed_rows.device
     G = torch.empty(((M + 3) // 4, N), dtype=torch.uint8, device=dev)
     nbytes = query_size("adx_bed_workspace_bytes", M, N)
-    ws = Workspace.get(dev, nbytes)
+    ws = Workspace.get(dev, nbytes, "bed")
     flipped = torch.zeros(1, dtype=torch.int32, device=dev)
     call("adx_bed_to_packed", bed_rows.data_ptr(), M, N, G.data_ptr(), flipped.data_ptr(),
          ws.data_ptr(), ws.numel(), _stream(dev))

@@ -218,6 +218,14 @@ int adx_cv_deviance_hash(const uint8_t* G0, int64_t M, int64_t N, int K, const d
                          const double* Q, uint64_t seed, int n_folds, int fold, double* out,
                          void* workspace, size_t workspace_bytes, void* stream);
 
+/* ---------------------------------------------------------------- outputs (host)
+ * Writes a float64 [rows][cols] HOST matrix as text, "%.18e" values separated by single
+ * spaces, one row per line: byte for byte np.savetxt(path, X, delimiter=' '), the
+ * reference's .Q/.P writer (write_outputs, adamixture/src/utils.py:252-273). threads <= 0:
+ * all hardware threads. */
+int adx_write_text_matrix(const char* path, const double* X, int64_t rows, int64_t cols,
+                          int threads);
+
 #ifdef __cplusplus
 }
 #endif

@@ -59,3 +59,8 @@ def demo_gpu():
 @pytest.fixture(scope="session")
 def cv_proj():
     return _load("cv_proj")
+
+
+@pytest.fixture(scope="session")
+def align_golden():
+    return _load("align")

@@ -3,7 +3,7 @@
 Run from the repository root, in a tree that has the reference sources and the
 compiled reference modules (``make -C oracle``):
 
-    python tests/golden/make_golden.py [edge synth demo demo_gpu solvers cv_proj]
+    python tests/golden/make_golden.py [edge synth demo demo_gpu solvers cv_proj align]
 
 What it records (all from the reference's own code, imported from its source tree;
 its ``torch.compile`` wrappers run eagerly as float64 torch code on the CPU, with the
@@ -24,6 +24,7 @@ CUDA unpack op replaced by a bit-shift unpacker of the same packed layout):
   Adam-EM results).
 * ``solvers.npz``: the reference's CPU BVLS (K = 1..64), gradient/Hessian and SQP
   outputs on seeded problems.
+* ``align.npz``: the reference's cluster alignment across K on seeded Q matrices.
 * ``cv_proj.npz``: the reference's cross-validation index (5 folds, seed 42) and fold
   rules, and its Adam-EM and SQP + ZAL projections, on a seeded cohort (N=90, M=700, K=3).
 """
@@ -259,8 +260,28 @@ def cv_proj(em, utils):
     print("cv_proj.npz cv_index", rec["cv_index"])
 
 
+def align():
+    """The reference's cluster alignment across K (plot.py align_clusters_clumppling) on
+    seeded Q matrices of equal, larger and smaller K."""
+    refmods.import_reference()
+    from adamixture.src.plot import align_clusters_clumppling
+
+    rng = np.random.default_rng(77)
+    rec = {}
+    for c, (Kr, Kq) in enumerate([(3, 3), (3, 4), (4, 6), (5, 4), (7, 7), (2, 5)]):
+        base = rng.dirichlet(np.full(max(Kr, Kq), 0.4), 200)
+        ref = base[:, :Kr] / base[:, :Kr].sum(1, keepdims=True)
+        perm = rng.permutation(Kq)
+        q = np.clip(base[:, :Kq] + rng.normal(0, 0.02, (200, Kq)), 1e-5, None)[:, perm]
+        q /= q.sum(1, keepdims=True)
+        rec[f"c{c}_ref"], rec[f"c{c}_query"] = ref, q
+        rec[f"c{c}_perm"] = np.asarray(align_clusters_clumppling(ref, q))
+    np.savez_compressed(OUT / "align.npz", **rec)
+    print("align.npz", len(rec))
+
+
 if __name__ == "__main__":
-    which = set(sys.argv[1:]) or {"edge", "synth", "demo", "demo_gpu", "solvers", "cv_proj"}
+    which = set(sys.argv[1:]) or {"edge", "synth", "demo", "demo_gpu", "solvers", "cv_proj", "align"}
     if which & {"edge", "synth", "demo", "cv_proj"}:
         em, utils = reference()
         if "edge" in which:
@@ -275,3 +296,5 @@ if __name__ == "__main__":
         demo_gpu()
     if "solvers" in which:
         solvers()
+    if "align" in which:
+        align()
