@@ -28,6 +28,7 @@ SIGNATURES: dict[str, list] = {
     "adx_unpack_center_f32": [P, I64, I64, I64, I64, I64, I64, P, P, P],
     "adx_allele_frequency": [P, I64, I64, P, P],
     "adx_sample_counts": [P, I64, I64, P, P],
+    "adx_sample_het_counts": [P, I64, I64, P, P],
     "adx_bed_workspace_bytes": [I64, I64, P],
     "adx_bed_to_packed": [P, I64, I64, P, P, P, c_size_t, P],
     "adx_simulate_packed": [P, P, I64, I64, c_int, c_uint64, c_uint64, c_uint32, P, P],
@@ -59,6 +60,11 @@ SIGNATURES: dict[str, list] = {
     "adx_cv_deviance_list": [P, I64, I64, c_int, P, P, P, I64, P, P, c_size_t, P],
     "adx_cv_deviance_hash": [P, I64, I64, c_int, P, P, c_uint64, c_int, c_int, P, P, c_size_t, P],
     "adx_write_text_matrix": [ctypes.c_char_p, P, I64, I64, c_int],
+    "adx_mlp_workspace_bytes": [I64, c_int, P],
+    "adx_mlp_forward": [P, P, P, P, P, P, P, P, I64, c_int, P, P, c_size_t, P],
+    "adx_mlp_backward": [P, P, P, P, I64, c_int, P, P, P, P, P, P, P, P, c_size_t, P],
+    "adx_mlp_adam": [P, P, P, P, P, I64, ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float,
+                     c_int, P],
 }
 _RESTYPE = {"adx_version": ctypes.c_char_p, "adx_last_error": ctypes.c_char_p}
 

@@ -4,7 +4,7 @@
     python -m adamixture_b200 --k 8 --data_path cohort.bed --save_dir out --name run --device gpu
 
 Options of the reference that concern other devices or the plotting stack are accepted;
-``--precision`` (f64 | f32 | bf16 | auto) selects the Adam-EM E-step arithmetic.
+``--precision`` (f64 | f32 | bf16 | mixed | auto) selects the Adam-EM E-step arithmetic.
 """
 from __future__ import annotations
 
@@ -21,7 +21,9 @@ def parse_args(argv: list[str]) -> argparse.Namespace:
     p.add_argument("--beta2", type=float, default=0.88)
     p.add_argument("--reg_adam", type=float, default=1e-8)
     p.add_argument("--algorithm", choices=["brqn", "adamem"], default="brqn")
-    p.add_argument("--init", choices=["em", "als"], default="als")
+    p.add_argument("--init", choices=["em", "als", "mlp"], default="als",
+                   help="initialisation: random + EM priming, SVD + ALS, or the learned warm start "
+                        "on top of SVD + ALS (Adam-EM only; kept only if no worse than plain EM)")
     p.add_argument("--em_init_steps", type=int, default=5, help=argparse.SUPPRESS)
     p.add_argument("--Q_hist", type=int, default=3, help=argparse.SUPPRESS)
     p.add_argument("--lr_decay", type=float, default=0.5)
@@ -56,7 +58,7 @@ def parse_args(argv: list[str]) -> argparse.Namespace:
     p.add_argument("--labels2")
     p.add_argument("--labels3")
     p.add_argument("--colors")
-    p.add_argument("--precision", choices=["f64", "f32", "bf16", "auto"], default=None)
+    p.add_argument("--precision", choices=["f64", "f32", "bf16", "mixed", "auto"], default=None)
     a = p.parse_args(argv)
     if a.device != "gpu":
         p.error("this build runs on the GPU only (--device gpu)")

@@ -106,6 +106,24 @@ __global__ void sample_counts_kernel(const uint8_t* __restrict__ G, int64_t M, i
   atomicAdd(q_bat + i, 2.0 * (double)(snps - (int64_t)miss));
 }
 
+// Heterozygous genotype (g = 1, bits 01) count per sample, same partition and exact
+// integer-valued float64 atomics as sample_counts_kernel; padding bits are 00 (g = 0).
+__global__ void het_counts_kernel(const uint8_t* __restrict__ G, int64_t M, int64_t N,
+                                  int64_t rows_per_part, double* __restrict__ het) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  const int64_t rows = (M + 3) >> 2;
+  const int64_t r0 = (int64_t)blockIdx.y * rows_per_part;
+  const int64_t r1 = min(rows, r0 + rows_per_part);
+  if (r0 >= r1) return;
+  unsigned long long h = 0;
+  for (int64_t r = r0; r < r1; ++r) {
+    const uint32_t b = G[r * N + i];
+    h += __popc(b & ~(b >> 1) & 0x55u);
+  }
+  atomicAdd(het + i, (double)h);
+}
+
 // ---------------------------------------------------------------- synthetic sampler
 
 __device__ __forceinline__ uint64_t splitmix64(uint64_t z) {
@@ -273,6 +291,23 @@ extern "C" int adx_sample_counts(const uint8_t* G, int64_t M, int64_t N, double*
   cudaStream_t st = as_stream(stream);
   ADX_CUDA_TRY(cudaMemsetAsync(q_bat, 0, (size_t)N * sizeof(double), st));
   sample_counts_kernel<<<dim3((unsigned)xblocks, (unsigned)parts), threads, 0, st>>>(G, M, N, rpp, q_bat);
+  ADX_LAUNCH_CHECK();
+  return ADX_OK;
+}
+
+extern "C" int adx_sample_het_counts(const uint8_t* G, int64_t M, int64_t N, double* het, void* stream) {
+  if (M <= 0 || N <= 0 || !G || !het) { adx_set_message("adx_sample_het_counts: bad arguments"); return ADX_ERR_ARG; }
+  const int64_t rows = (M + 3) >> 2;
+  const int threads = 256;
+  const int64_t xblocks = ceil_div(N, threads);
+  int64_t parts = ceil_div((int64_t)sm_count() * 8, xblocks);
+  parts = parts < 1 ? 1 : (parts > rows ? rows : parts);
+  parts = parts > 65535 ? 65535 : parts;
+  const int64_t rpp = ceil_div(rows, parts);
+  parts = ceil_div(rows, rpp);
+  cudaStream_t st = as_stream(stream);
+  ADX_CUDA_TRY(cudaMemsetAsync(het, 0, (size_t)N * sizeof(double), st));
+  het_counts_kernel<<<dim3((unsigned)xblocks, (unsigned)parts), threads, 0, st>>>(G, M, N, rpp, het);
   ADX_LAUNCH_CHECK();
   return ADX_OK;
 }

@@ -10,7 +10,8 @@ the arithmetic.
 
 E-step arithmetic (``precision``): ``"f64"`` reproduces the reference's float64 path;
 ``"f32"`` forms ratios and partial sums in float32 (float64 cross-block sums);
-``"bf16"`` is the tensor-core form for K >= 8. ``set_precision`` sets the default
+``"bf16"`` is the tensor-core form for K >= 8; ``"mixed"`` runs tensor-core sweeps until
+the first plateau and float32 sweeps after it. ``set_precision`` sets the default
 (environment: ``ADX_PRECISION``); the default policy ("auto") is ``"bf16"`` for
 8 <= K <= 16 and ``"f32"`` otherwise.
 """
@@ -30,9 +31,9 @@ _PRECISION = os.environ.get("ADX_PRECISION", "auto")
 
 
 def set_precision(p: str) -> None:
-    """Default E-step arithmetic: "f64", "f32", "bf16" or "auto"."""
+    """Default E-step arithmetic: "f64", "f32", "bf16", "mixed" or "auto"."""
     global _PRECISION
-    if p != "auto":
+    if p not in ("auto", "mixed"):
         ops.precision_code(p)
     _PRECISION = p
 
@@ -42,9 +43,10 @@ TC_MIN_K, TC_MAX_K = 8, 16
 
 def resolve_precision(K: int, precision: str | None = None) -> str:
     """The E-step arithmetic for this K. "auto": tensor cores (BF16 operands, FP32
-    accumulation) for 8 <= K <= 16, float32 otherwise."""
+    accumulation) for 8 <= K <= 16, float32 otherwise. "mixed" resolves to the first
+    phase's arithmetic here (the optimiser switches to float32 at the first plateau)."""
     p = precision or _PRECISION
-    if p == "auto":
+    if p in ("auto", "mixed"):
         return "bf16" if TC_MIN_K <= K <= TC_MAX_K else "f32"
     if p == "bf16" and K > TC_MAX_K:
         raise ValueError(f"the tensor-core E-step supports K <= {TC_MAX_K} (got K={K}); use 'f32'")
@@ -167,8 +169,11 @@ def _optimize_parameters_gpu_once(G, P, Q, lr, beta1, beta2, reg_adam, max_iter,
     the primed point as the first best, then ``max_iter`` iterations with a check every
     ``check`` iterations. The reference's second priming E-step, whose result it never
     uses (:322), is skipped: it changes no state. ``trace`` (a list) receives
-    ``(iteration, loglik)`` at each check.
+    ``(iteration, loglik)`` at each check. ``precision="mixed"``: tensor-core (BF16) sweeps
+    until the first plateau (``patience`` checks without a new best), float32 sweeps after
+    it, with the same Adam state and learning rate.
     """
+    mixed = (precision or _PRECISION) == "mixed"
     opt = EMAdamOptimizer(P.shape, Q.shape, lr, beta1, beta2, reg_adam, device, precision)
     prec = opt.precision
     ll_prec = "f64" if prec == "f64" else "f32"
@@ -209,6 +214,14 @@ def _optimize_parameters_gpu_once(G, P, Q, lr, beta1, beta2, reg_adam, max_iter,
                 wait_lr = 0
             else:
                 wait_lr += 1
+                if wait_lr >= patience and mixed and prec != "f32":
+                    # mixed precision: the first plateau ends the BF16 phase; the same Adam
+                    # state continues with float32 sweeps (same float32 P/Q shadows)
+                    prec = opt.precision = "f32"
+                    ws = ops.Workspace.get(G.device, ops.em_workspace_bytes(M, N, K, prec))
+                    log.info("    Plateau in the BF16 phase: continuing with float32 E-steps.")
+                    wait_lr = 0
+                    continue
                 if wait_lr >= patience:
                     old = opt.lr
                     opt.lr = max(opt.lr * lr_decay, min_lr)

@@ -116,6 +116,14 @@ def sample_counts(G: torch.Tensor, M: int) -> torch.Tensor:
     return q
 
 
+def sample_het_counts(G: torch.Tensor, M: int) -> torch.Tensor:
+    """Heterozygous genotype count per sample (float64, exact)."""
+    _check(G, "G", torch.uint8)
+    h = torch.empty(G.shape[1], dtype=torch.float64, device=G.device)
+    call("adx_sample_het_counts", G.data_ptr(), M, G.shape[1], h.data_ptr(), _stream(G.device))
+    return h
+
+
 def bed_to_packed(bed_rows: torch.Tensor, N: int, M: int) -> torch.Tensor:
     """PLINK BED rows ``[M, ceil(N/4)]`` (device) -> packed ``[ceil(M/4), N]``, flipped
     0<->2 when the mean dosage/2 is >= 0.5 (the reference reader's rule)."""

@@ -94,6 +94,16 @@ def train_k(G, N: int, M: int, K: int, U_max, S_max, V_max, f, seed: int, lr: fl
             init_original: str = "em", em_init_steps: int = 5, P_init=None, Q_init=None,
             precision: str | None = None):
     """Train one K from the shared SVD (adamixture.py:253-383, GPU branch): ``(P, Q)``."""
+    if P_init is None and init_original == "mlp" and not original:
+        # learned warm start, kept only if EM from it is no worse than plain EM from the
+        # ALS start (both run; the better model is returned)
+        from ..model import warm_start as ws
+
+        net = ws.WarmStartMLP.load(ws.DEFAULT_WEIGHTS, device_obj)
+        r = ws.warm_start_fit(net, G, N, M, K, seed, precision)
+        log.info(f"    Warm start {'kept' if r['kept_warm'] else 'rejected'}: log-likelihood "
+                 f"{r['loglik_warm']:.1f} (warm) vs {r['loglik_plain']:.1f} (plain).")
+        return r["P"], r["Q"]
     if P_init is not None and Q_init is not None:
         P, Q = P_init, Q_init
     else:

@@ -66,6 +66,10 @@ int adx_allele_frequency(const uint8_t* G, int64_t M, int64_t N, float* f, void*
 /* q_bat_i = 2 * #observed SNPs of sample i (float64): the per-sample count that the
  * reference re-accumulates on every E-step (adamixture/model/em_adam_gpu.py:76, 196). */
 int adx_sample_counts(const uint8_t* G, int64_t M, int64_t N, double* q_bat, void* stream);
+/* Heterozygous (g = 1) genotype count per sample, float64 [N] (exact integers); with
+ * adx_sample_counts it gives the warm-start network's heterozygosity feature. No
+ * counterpart in the reference. */
+int adx_sample_het_counts(const uint8_t* G, int64_t M, int64_t N, double* het, void* stream);
 
 /* PLINK BED rows bed[M][ceil(N/4)] (SNP-major, LUT [2,3,1,0]) -> packed G, then the
  * reference's 0<->2 flip when the mean dosage/2 is >= 0.5. `flipped` (device int) receives
@@ -225,6 +229,27 @@ int adx_cv_deviance_hash(const uint8_t* G0, int64_t M, int64_t N, int K, const d
  * all hardware threads. */
 int adx_write_text_matrix(const char* path, const double* X, int64_t rows, int64_t cols,
                           int threads);
+
+/* ---------------------------------------------------------------- warm-start network
+ * No counterpart in the reference (a new component of this build). A per-sample network
+ * 33 -> 256 -> 256 -> K (K <= 16), GELU hidden layers, output softmax(f(x) + prior) with
+ * prior [B][K] optional (log of the ALS memberships, so an untrained network reproduces the
+ * ALS start). Weights BF16 (uint16 bit patterns) [out][in], biases and activations float32.
+ * adx_mlp_forward keeps the activations in the workspace; adx_mlp_backward (same X, same
+ * workspace, right after the forward) writes the mean cross-entropy against soft targets T
+ * to *loss (device float) and every weight/bias gradient (float32). adx_mlp_adam: one Adam
+ * step (bias-corrected, step t >= 1) on a float32 master, refreshing its BF16 copy. */
+int adx_mlp_workspace_bytes(int64_t B, int K, size_t* bytes);
+int adx_mlp_forward(const float* X, const float* prior, const uint16_t* W1, const float* b1,
+                    const uint16_t* W2, const float* b2, const uint16_t* W3, const float* b3,
+                    int64_t B, int K, float* Q_out, void* workspace, size_t workspace_bytes,
+                    void* stream);
+int adx_mlp_backward(const float* X, const float* T, const uint16_t* W2, const uint16_t* W3,
+                     int64_t B, int K, float* dW1, float* db1, float* dW2, float* db2,
+                     float* dW3, float* db3, float* loss, void* workspace,
+                     size_t workspace_bytes, void* stream);
+int adx_mlp_adam(float* w, uint16_t* w_bf16, const float* g, float* m, float* v, int64_t n,
+                 float lr, float beta1, float beta2, float eps, int t, void* stream);
 
 #ifdef __cplusplus
 }

@@ -108,3 +108,27 @@ def test_tc_converged_loglik(ops, name, request):
     ref = float(d["conv_loglik"])
     print(name, "bf16 converged loglik", L, "reference", ref, "rel", abs(L - ref) / abs(ref))
     assert abs(L - ref) <= 1e-4 * abs(ref)
+
+
+@pytest.mark.parametrize("name", ["demo", "synth"])
+def test_mixed_precision_reaches_the_float32_fit(ops, name, request):
+    # BF16 tensor-core sweeps to the first plateau, float32 after it: the converged
+    # log-likelihood matches the plain float32 run's within 1e-6 relative
+    import time
+
+    from adamixture_b200.model.em_adam_gpu import loglikelihood_gpu, optimize_parameters_gpu
+
+    d = request.getfixturevalue(name)
+    M, N, K = int(d["M"]), int(d["N"]), int(d["K"])
+    G = dev_t(d["packed"])
+    out = {}
+    for prec in ("f32", "mixed"):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        P, Q = optimize_parameters_gpu(G, dev_t(d["P0"]), dev_t(d["Q0"]), 0.005, 0.80, 0.88, 1e-8, 10000, 5, K,
+                                       M, N, 0.5, 1e-4, 3, 0.1, G.device, 8192, 512, precision=prec)
+        torch.cuda.synchronize()
+        out[prec] = (loglikelihood_gpu(G, P, Q, M, N, 8192, G.device, 512), time.perf_counter() - t0)
+    print(name, "f32", out["f32"], "mixed", out["mixed"])
+    L32, Lm = out["f32"][0], out["mixed"][0]
+    assert abs(Lm - L32) <= 1e-6 * abs(L32)
