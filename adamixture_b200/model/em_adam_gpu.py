@@ -169,7 +169,8 @@ def _optimize_parameters_gpu_once(G, P, Q, lr, beta1, beta2, reg_adam, max_iter,
     the primed point as the first best, then ``max_iter`` iterations with a check every
     ``check`` iterations. The reference's second priming E-step, whose result it never
     uses (:322), is skipped: it changes no state. ``trace`` (a list) receives
-    ``(iteration, loglik)`` at each check. ``precision="mixed"``: tensor-core (BF16) sweeps
+    ``(iteration, loglik, seconds since the start)`` at each check (host clock after the
+    check's read-back, so the device work up to it is included). ``precision="mixed"``: tensor-core (BF16) sweeps
     until the first plateau (``patience`` checks without a new best), float32 sweeps after
     it, with the same Adam state and learning rate.
     """
@@ -193,6 +194,7 @@ def _optimize_parameters_gpu_once(G, P, Q, lr, beta1, beta2, reg_adam, max_iter,
         return L
 
     ts = time.time()
+    t_start = time.perf_counter()
     opt.fused_iteration(G, P, Q, P32, Q32, M, ws)
     log.info(f"    Performed priming iteration... ({time.time() - ts:.1f}s)\n")
     L_best = loglik()
@@ -204,7 +206,7 @@ def _optimize_parameters_gpu_once(G, P, Q, lr, beta1, beta2, reg_adam, max_iter,
         if (it + 1) % check == 0:
             L_cur = loglik()
             if trace is not None:
-                trace.append((it + 1, L_cur))
+                trace.append((it + 1, L_cur, time.perf_counter() - t_start))
             log.info(f"    Iteration {it+1}, Log-likelihood: {L_cur:.1f}, Time: {time.time() - ts:.3f}s")
             ts = time.time()
             if L_cur > L_best + tol_adam:

@@ -282,7 +282,7 @@ def training_set(cohorts, device, precision=None):
 
 def iterations_to_reach(trace, target: float, rel: float = 1e-6):
     """First traced iteration whose log-likelihood is within ``rel`` of ``target``."""
-    for it, L in trace:
+    for it, L, *_ in trace:
         if L >= target - rel * abs(target):
             return it
     return None
@@ -312,8 +312,8 @@ def warm_start_fit(net: WarmStartMLP, G, N: int, M: int, K: int, seed: int = 42,
         "loglik_plain": L_p, "loglik_warm": L_w, "kept_warm": bool(keep),
         "seconds_plain": t_plain, "seconds_warm": t_warm,
         # traced values share the runs' log-likelihood arithmetic: compare within it
-        "iters_plain": iterations_to_reach(tr_p, max(L for _, L in tr_p)) if tr_p else None,
-        "iters_warm_to_plain": iterations_to_reach(tr_w, max(L for _, L in tr_p)) if tr_p else None,
+        "iters_plain": iterations_to_reach(tr_p, max(e[1] for e in tr_p)) if tr_p else None,
+        "iters_warm_to_plain": iterations_to_reach(tr_w, max(e[1] for e in tr_p)) if tr_p else None,
         "loglik_init_als": loglikelihood_gpu(G, P_als, Q_als, M, N, 8192, G.device, 256),
         "loglik_init_warm": loglikelihood_gpu(G, P_w0, Q_w0, M, N, 8192, G.device, 256),
         "loglik_init_als_P_warm_Q": loglikelihood_gpu(G, P_als, Q_w0, M, N, 8192, G.device, 256),

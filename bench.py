@@ -408,6 +408,70 @@ def run_e2e(args, G_dev, P0, Q0, M, N, K, prec, dev):
                     "best P/Q copied to the host"}
 
 
+def run_converge(args, cfg):
+    """Time to the converged log-likelihood at the config: from the reference's default
+    start (randomized SVD + ALS), plain float32 Adam-EM to its stop, then BF16, mixed
+    (BF16 then float32) and the learned warm start + mixed, each timed to the first check
+    within 1e-6 relative of the plain float32 run's best log-likelihood. One JSON line."""
+    import torch
+
+    from adamixture_b200 import ops
+    from adamixture_b200.model import warm_start as ws
+    from adamixture_b200.model.em_adam_gpu import loglikelihood_gpu, optimize_parameters_gpu
+    from adamixture_b200.src.simulate import make_cohort
+
+    dev = torch.device("cuda", 0)
+    N, M, K = cfg["N"], cfg["M"], cfg["K"]
+    coh = make_cohort(N, M, K, cfg["F"], cfg["alpha"], cfg["miss"], cfg["seed"])
+    Pq = torch.from_numpy(coh.Pq.astype(np.int32)).to(dev)
+    Qq = torch.from_numpy(coh.Qq.astype(np.int32)).to(dev)
+    G = ops.simulate_packed(Pq, Qq, coh.miss_q, coh.keys)
+    del Pq, Qq
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    U, S, V, P0, Q0 = ws.init_als(G, N, M, K, seed=42)
+    torch.cuda.synchronize()
+    t_init = time.perf_counter() - t0
+    runs = {}
+
+    def fit(name, P_start, Q_start, prec, extra_s=0.0):
+        tr = []
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        P, Q = optimize_parameters_gpu(G, P_start.clone(), Q_start.clone(), HP["lr"], HP["beta1"], HP["beta2"],
+                                       HP["eps"], args.converge_max_iter, CHECK, K, M, N, 0.5, 1e-4, 3, 0.1, dev,
+                                       8192, 256, precision=prec, trace=tr)
+        torch.cuda.synchronize()
+        el = time.perf_counter() - t
+        L = loglikelihood_gpu(G, P, Q, M, N, 8192, dev, 256)
+        runs[name] = {"precision": prec, "seconds": el + extra_s, "iterations": tr[-1][0] if tr else 0,
+                      "loglik": L, "trace": tr}
+
+    fit("plain_f32", P0, Q0, "f32")
+    target = max(e[1] for e in runs["plain_f32"]["trace"])
+    fit("bf16", P0, Q0, "bf16" if 8 <= K <= 16 else "f32")
+    fit("mixed", P0, Q0, "mixed")
+    net = ws.WarmStartMLP.load(ws.DEFAULT_WEIGHTS, dev)
+    torch.cuda.synchronize()
+    t = time.perf_counter()
+    Pw, Qw = ws.predict(net, G, M, U, S, V, Q0, P0)
+    torch.cuda.synchronize()
+    fit("warm_mixed", Pw, Qw, "mixed", extra_s=time.perf_counter() - t)
+    out = {}
+    for name, r in runs.items():
+        reach = next(((it, sec) for it, L, sec in r["trace"] if L >= target - 1e-6 * abs(target)), None)
+        out[name] = {"precision": r["precision"], "seconds_to_stop": r["seconds"], "iterations_to_stop": r["iterations"],
+                     "loglik": r["loglik"], "rel_gap_to_plain_f32": (runs["plain_f32"]["loglik"] - r["loglik"])
+                     / abs(runs["plain_f32"]["loglik"]),
+                     "iterations_to_target": reach[0] if reach else None,
+                     "seconds_to_target": reach[1] if reach else None}
+    line = {"metric": "time-to-converged loglik", "config": {"workload": cfg["workload"],
+            "start": "randomized SVD (k=max(K,16), power 5) + ALS, seed 42", "check_every": CHECK,
+            "max_iter": args.converge_max_iter, "target": "first check within 1e-6 relative of the plain float32 "
+            "run's best (traced) log-likelihood"}, "init_seconds": t_init, "runs": out}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -419,6 +483,9 @@ def main():
     ap.add_argument("--cpu-snps", dest="cpu_snps", type=int, default=4096)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--converge", action="store_true",
+                    help="instead of the throughput line, time runs to the converged log-likelihood")
+    ap.add_argument("--converge-max-iter", dest="converge_max_iter", type=int, default=300)
     args = ap.parse_args()
     if args.warmup < 3:
         print("bench.py: --warmup must be >= 3", file=sys.stderr)
@@ -429,6 +496,10 @@ def main():
     cfg = CONFIGS[args.config]
     if args.impl == "reference":
         run_reference_arm(args, cfg, rank)
+        return
+    if args.converge:
+        if rank == 0:
+            run_converge(args, cfg)
         return
     run_gpu_arm(args, cfg, rank, world, local_rank)
 
