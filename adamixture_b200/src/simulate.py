@@ -123,6 +123,14 @@ class Cohort:
         return out
 
 
+def shard_keys(keys: tuple[int, int], j0: int, N: int) -> tuple[int, int]:
+    """Sampler keys that make SNP rows [j0, ...) of a cohort come out of a sampler started
+    at row 0: the stream of entry (j, i) is splitmix64((j N + i) * GOLDEN + key), so
+    shifting the keys by j0 N GOLDEN (mod 2^64) shifts j by j0."""
+    shift = (int(j0) * int(N) * int(GOLDEN)) % (1 << 64)
+    return ((int(keys[0]) + shift) % (1 << 64), (int(keys[1]) + shift) % (1 << 64))
+
+
 def make_cohort(N: int, M: int, K: int, F: float, alpha: float | tuple = 0.5,
                 miss: float = 0.01, seed: int = 0) -> Cohort:
     """Draw the true P and Q for a cohort.

@@ -229,45 +229,71 @@ def run_gpu_arm(args, cfg, rank, world, local_rank):
     torch.cuda.set_device(dev)
     N, M, K = cfg["N"], cfg["M"], cfg["K"]
     prec = resolve_precision(K, args.precision)
-    if world > 1:
+    sharded = world > 1 or args.shard
+    if sharded:
+        import datetime
+
         import torch.distributed as dist
-        dist.init_process_group("nccl", device_id=dev)
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        os.environ.setdefault("MASTER_PORT", "29531")
+        os.environ.setdefault("RANK", str(rank))
+        os.environ.setdefault("WORLD_SIZE", str(world))
+        dist.init_process_group("nccl", device_id=dev, timeout=datetime.timedelta(minutes=10))
+
+    from adamixture_b200.model.em_adam_dist import CudaBackend, ShardedAdamEM, shard_rows
+    from adamixture_b200.src.simulate import shard_keys
 
     coh = make_cohort(N, M, K, cfg["F"], cfg["alpha"], cfg["miss"], cfg["seed"])
-    Pq = torch.from_numpy(coh.Pq.astype(np.int32)).to(dev)
+    # this rank's SNP rows (all of them on one GPU); exactly that slice of the cohort
+    j0, j1 = shard_rows(M, world, rank) if world > 1 else (0, M)
+    M_loc = j1 - j0
+    Pq = torch.from_numpy(coh.Pq[j0:j1].astype(np.int32)).to(dev)
     Qq = torch.from_numpy(coh.Qq.astype(np.int32)).to(dev)
-    G = ops.simulate_packed(Pq, Qq, coh.miss_q, coh.keys)
+    G = ops.simulate_packed(Pq, Qq, coh.miss_q, shard_keys(coh.keys, j0, N))
     del Pq, Qq
     rng = np.random.default_rng(cfg["seed"])
-    P0 = np.clip(rng.random((M, K)), 1e-5, 1 - 1e-5)
+    P0 = np.clip(rng.random((M, K)), 1e-5, 1 - 1e-5)[j0:j1].copy()
     Q0 = np.clip(rng.random((N, K)), 1e-5, 1 - 1e-5)
     Q0 /= Q0.sum(1, keepdims=True)
     P = torch.from_numpy(P0).to(dev)
     Q = torch.from_numpy(Q0).to(dev)
     P32, Q32 = P.float(), Q.float()
-    opt = EMAdamOptimizer(P.shape, Q.shape, HP["lr"], HP["beta1"], HP["beta2"], HP["eps"], dev, prec)
-    ws = ops.Workspace.get(dev, ops.em_workspace_bytes(M, N, K, prec))
+    ws = ops.Workspace.get(dev, ops.em_workspace_bytes(M_loc, N, K, prec))
     llp = "f64" if prec == "f64" else "f32"
     Pll, Qll = (P, Q) if llp == "f64" else (P32, Q32)
     launches = {"n": 0}
 
-    # kernels per fused iteration: sweep (+ the BF16 copy of Q for the tensor-core sweep)
-    # and the update kernel; per check: the log-likelihood kernel and its final sum
-    per_iter = 3 if prec == "bf16" else 2
+    if not sharded:
+        # kernels per fused iteration: sweep (+ the BF16 copy of Q for the tensor-core sweep)
+        # and the update kernel; per check: the log-likelihood kernel and its final sum
+        opt = EMAdamOptimizer(P.shape, Q.shape, HP["lr"], HP["beta1"], HP["beta2"], HP["eps"], dev, prec)
+        per_iter = 3 if prec == "bf16" else 2
 
-    def one_step(it):
-        opt.fused_iteration(G, P, Q, P32, Q32, M, ws)
-        launches["n"] += per_iter
-        if (it + 1) % CHECK == 0:
-            float(ops.loglik_device(G, Pll, Qll, M, llp).item())
-            launches["n"] += 2
+        def one_step(it):
+            opt.fused_iteration(G, P, Q, P32, Q32, M, ws)
+            launches["n"] += per_iter
+            if (it + 1) % CHECK == 0:
+                float(ops.loglik_device(G, Pll, Qll, M, llp).item())
+                launches["n"] += 2
+    else:
+        # SNP-sharded: local sweep + statistics, all-reduce of T, targets, Adam (Q replicated)
+        run = ShardedAdamEM(G, P, Q, M_loc, K, HP["beta1"], HP["beta2"], HP["eps"], HP["lr"],
+                            backend=CudaBackend(prec))
+        per_iter = (3 if prec == "bf16" else 2) + 2
+
+        def one_step(it):
+            run.iteration()
+            launches["n"] += per_iter
+            if (it + 1) % CHECK == 0:
+                run.loglik()
+                launches["n"] += 2
 
     torch.cuda.synchronize()
     for it in range(args.warmup):
         one_step(it)
     torch.cuda.synchronize()
     launches["n"] = 0
-    if world > 1:
+    if sharded:
         torch.distributed.barrier()
     torch.cuda.synchronize()
     uuid = None
@@ -284,45 +310,48 @@ def run_gpu_arm(args, cfg, rank, world, local_rank):
         e1.record(stream)
         torch.cuda.synchronize()
     ms = e0.elapsed_time(e1)
-    if world > 1:
+    if sharded:
         t = torch.tensor([ms], device=dev)
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         ms = float(t.item())
     ms_per_step = ms / args.steps
 
-    # roofline: the sweep kernel alone, CUDA events on its stream
-    Pin, Qin = (P, Q) if prec == "f64" else (P32, Q32)
+    # roofline: the sweep kernel alone (this rank's rows), CUDA events on its stream
+    Pin, Qin = (P, Q) if prec == "f64" else (P.float(), Q.float())
     reps = max(3, min(10, args.steps))
-    ops.em_sweep(G, Pin, Qin, M, prec, ws)
+    ops.em_sweep(G, Pin, Qin, M_loc, prec, ws)
     torch.cuda.synchronize()
     s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     s0.record(stream)
     for _ in range(reps):
-        ops.em_sweep(G, Pin, Qin, M, prec, ws)
+        ops.em_sweep(G, Pin, Qin, M_loc, prec, ws)
     s1.record(stream)
     torch.cuda.synchronize()
     sweep_ms = s0.elapsed_time(s1) / reps
     hbm, peak_kind = peaks()
-    ab = alg_bytes(M, N, K)
+    ab = alg_bytes(M_loc, N, K)
     achieved = ab / (sweep_ms * 1e-3) / 1e9
     roof = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-            "frac": achieved / hbm, "traffic": traffic_per_launch(M, N, K, prec),
+            "frac": achieved / hbm, "traffic": traffic_per_launch(M_loc, N, K, prec),
             "kernel": "em_sweep_tc_kernel" if prec == "bf16" else f"em_sweep_kernel<{'double' if prec == 'f64' else 'float'},{ops_kmax(K)}>",
             "launch_ms": sweep_ms, "alg_bytes": ab, "peak_kind": peak_kind,
-            "entries_per_s": M * N / (sweep_ms * 1e-3)}
+            "entries_per_s": M_loc * N / (sweep_ms * 1e-3), "snp_rows_per_rank": M_loc}
     if prec == "bf16":
         # the contractions (h, 1-h, A, B, T: 8 M N K flops of useful work; K padded to 16 in
         # the MMAs) against the measured dense BF16 peak, for the tensor-core sweep
         tf = peaks_tensor()
-        flops = 8.0 * M * N * K
+        flops = 8.0 * M_loc * N * K
         roof["tensor"] = {"achieved_tflops": flops / (sweep_ms * 1e-3) / 1e12, "peak_tflops": tf,
                           "frac": flops / (sweep_ms * 1e-3) / 1e12 / tf if tf else None,
                           "flops_per_launch": flops}
 
     # e2e through the public API from pinned host buffers
     e2e = None
-    if not args.no_e2e and rank == 0:
-        e2e = run_e2e(args, G, P0, Q0, M, N, K, prec, dev)
+    if not args.no_e2e:
+        if not sharded:
+            e2e = run_e2e(args, G, P0, Q0, M, N, K, prec, dev)
+        else:
+            e2e = run_e2e_dist(args, G, P0, Q0, M_loc, N, K, prec, dev, world)
 
     cpu = None
     if not args.no_cpu and rank == 0 and world == 1:
@@ -340,12 +369,13 @@ def run_gpu_arm(args, cfg, rank, world, local_rank):
             "config": {"workload": cfg["workload"], "precision": prec, "check_every": CHECK,
                        "l2": "inputs (packed G) larger than L2; no flush",
                        "genotype_GBps": ((M + 3) // 4) * N / (ms_per_step * 1e-3) / 1e9,
-                       "parallelism": "single GPU" if world == 1 else f"{world} ranks"},
+                       "parallelism": "single GPU" if not sharded else
+                       f"SNP rows sharded over {world} rank(s) (one all-reduce of T per iteration)"},
             "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": launches["n"], "clocks": clk.summary(),
         }
         print(json.dumps(line), flush=True)
-    if world > 1:
+    if sharded:
         torch.distributed.destroy_process_group()
 
 
@@ -472,6 +502,41 @@ def run_converge(args, cfg):
     print(json.dumps(line), flush=True)
 
 
+def run_e2e_dist(args, G_dev, P0, Q0, M_loc, N, K, prec, dev, world):
+    """e2e at N GPUs: each rank's packed rows and P rows plus Q from pinned host memory,
+    ``optimize_parameters_dist`` for ``steps`` iterations, P rows and Q back to the host;
+    max over ranks of the wall time."""
+    import torch
+    import torch.distributed as dist
+
+    from adamixture_b200.model.em_adam_dist import CudaBackend, optimize_parameters_dist
+
+    G_host = torch.empty(G_dev.shape, dtype=torch.uint8, pin_memory=True)
+    G_host.copy_(G_dev)
+    P_host = torch.from_numpy(P0).pin_memory()
+    Q_host = torch.from_numpy(Q0).pin_memory()
+    dist.barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    Gd = G_host.to(dev, non_blocking=True)
+    Pd = P_host.to(dev, non_blocking=True)
+    Qd = Q_host.to(dev, non_blocking=True)
+    Pb, Qb = optimize_parameters_dist(Gd, Pd, Qd, HP["lr"], HP["beta1"], HP["beta2"], HP["eps"], args.steps, CHECK,
+                                      K, M_loc, N, 0.5, 1e-4, 3, 0.1, backend=CudaBackend(prec))
+    Pr, Qr = Pb.cpu(), Qb.cpu()
+    el = torch.tensor([time.perf_counter() - t0], device=dev)
+    dist.all_reduce(el, op=dist.ReduceOp.MAX)
+    el = float(el.item())
+    del Gd
+    iters = args.steps
+    return {"value": iters / el, "unit": UNIT,
+            "h2d_bytes_per_step": (G_host.numel() + P0.nbytes + Q0.nbytes) * world / iters,
+            "d2h_bytes_per_step": (Pr.numel() * 8 + Qr.numel() * 8) * world / iters,
+            "pinned": True, "seconds": el,
+            "note": "optimize_parameters_dist on every rank with max_iter=steps from pinned host shards; "
+                    "bytes summed over ranks; max over ranks of the wall time"}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -483,6 +548,8 @@ def main():
     ap.add_argument("--cpu-snps", dest="cpu_snps", type=int, default=4096)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--shard", action="store_true",
+                    help="use the SNP-sharded path (NCCL all-reduce of T) even on one GPU")
     ap.add_argument("--converge", action="store_true",
                     help="instead of the throughput line, time runs to the converged log-likelihood")
     ap.add_argument("--converge-max-iter", dest="converge_max_iter", type=int, default=300)
