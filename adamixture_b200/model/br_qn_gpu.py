@@ -48,10 +48,12 @@ def _v_kk(K: int, device) -> torch.Tensor:
 
 
 def _optimize_original_gpu_once(G, P, Q, max_iter, K, M, N, tol, Q_hist, patience, device,
-                                qn_projection="clamp", verbose=True):
+                                qn_projection="clamp", verbose=True, q_hook=None):
     """``qn_projection``: how the extrapolated point returns to the feasible set -- "clamp"
     (clamp and renormalise, the GPU reference, br_qn_gpu.py:341) or "simplex" (box for P,
-    simplex projection for Q, the CPU reference, adamixture/model/br_qn.py:157-158)."""
+    simplex projection for Q, the CPU reference, adamixture/model/br_qn.py:157-158).
+    ``q_hook(Q)``: applied in place to every new Q (both SQP updates and the extrapolated
+    point), as supervised mode snaps labelled rows (adamixture/src/supervised.py:602-760)."""
     dt = torch.float64
     v_kk = _v_kk(K, device)
     XtX_q = torch.zeros((N, K, K), dtype=dt, device=device)
@@ -76,7 +78,10 @@ def _optimize_original_gpu_once(G, P, Q, max_iter, K, M, N, tol, Q_hist, patienc
     def sqp_q(Pm, Qm):
         ops.grad_hess_q(G, Pm, Qm, M, XtX_q, Xtz_q)
         Xtz_q.neg_()
-        return ops.sqp_solve_q(XtX_q, Xtz_q, Qm, v_kk, N, K)
+        Qn = ops.sqp_solve_q(XtX_q, Xtz_q, Qm, v_kk, N, K)
+        if q_hook is not None:
+            q_hook(Qn)
+        return Qn
 
     def sqp_p(Pm, Qm):
         ops.grad_hess_p(G, Pm, Qm, M, XtX_p, Xtz_p)
@@ -122,6 +127,8 @@ def _optimize_original_gpu_once(G, P, Q, max_iter, K, M, N, tol, Q_hist, patienc
             ops.project_simplex_(Q_qn)
         else:
             _mapPQ_gpu(P_qn, Q_qn)
+        if q_hook is not None:
+            q_hook(Q_qn)
 
         ll_qn = logl(P_qn, Q_qn)
         if ll_qn > ll_prev:

@@ -64,3 +64,8 @@ def cv_proj():
 @pytest.fixture(scope="session")
 def align_golden():
     return _load("align")
+
+
+@pytest.fixture(scope="session")
+def supervised_golden():
+    return _load("supervised")

@@ -3,7 +3,7 @@
 Run from the repository root, in a tree that has the reference sources and the
 compiled reference modules (``make -C oracle``):
 
-    python tests/golden/make_golden.py [edge synth demo demo_gpu solvers cv_proj align]
+    python tests/golden/make_golden.py [edge synth demo demo_gpu solvers cv_proj align supervised]
 
 What it records (all from the reference's own code, imported from its source tree;
 its ``torch.compile`` wrappers run eagerly as float64 torch code on the CPU, with the
@@ -24,6 +24,8 @@ CUDA unpack op replaced by a bit-shift unpacker of the same packed layout):
   Adam-EM results).
 * ``solvers.npz``: the reference's CPU BVLS (K = 1..64), gradient/Hessian and SQP
   outputs on seeded problems.
+* ``supervised.npz``: the reference's supervised initialisation and its Adam-EM (GPU path,
+  run on the CPU) and SQP + ZAL (CPU path) fits on a cohort with 40 % labelled samples.
 * ``align.npz``: the reference's cluster alignment across K on seeded Q matrices.
 * ``cv_proj.npz``: the reference's cross-validation index (5 folds, seed 42) and fold
   rules, and its Adam-EM and SQP + ZAL projections, on a seeded cohort (N=90, M=700, K=3).
@@ -260,6 +262,41 @@ def cv_proj(em, utils):
     print("cv_proj.npz cv_index", rec["cv_index"])
 
 
+def supervised(em, utils):
+    """The reference's supervised mode on a seeded cohort with 40 % of the samples labelled:
+    its initialisation (supervised_entry.py:309-315), its GPU-path Adam-EM run on the CPU
+    and its CPU SQP + ZAL run."""
+    from adamixture.src import supervised as sup
+    from adamixture_b200.src.simulate import make_cohort
+
+    sup.utils.get_unpacker = utils.get_unpacker
+    N, M, K = 120, 900, 3
+    coh = make_cohort(N, M, K, F=0.1, alpha=0.3, miss=0.02, seed=41)
+    G = np.ascontiguousarray(coh.genotypes())
+    rng_lab = np.random.default_rng(4)
+    y = np.where(rng_lab.random(N) < 0.4, np.argmax(coh.Q, 1) + 1, 0).astype(np.int64)
+    rng = np.random.default_rng(42)
+    P = sup.init_p_supervised(G, y, K, M)
+    P_packed = sup.init_p_supervised_packed(torch.from_numpy(coh.packed()), y, K, M)
+    Q = rng.random(size=(N, K)).astype(np.float64)
+    sup.init_q_supervised(Q, y, K)
+    dev = torch.device("cpu")
+    Pa, Qa = sup.optimize_supervised_gpu(
+        torch.from_numpy(coh.packed()), torch.from_numpy(P.copy()), torch.from_numpy(Q.copy()), y,
+        HP["lr"], HP["beta1"], HP["beta2"], HP["reg_adam"], 10000, HP["check"], M, HP["lr_decay"],
+        HP["min_lr"], HP["patience"], HP["tol"], dev, 8192, 1)
+    # the first 40 iterations with every check an improvement: P_best is the 40th iterate
+    P40, Q40 = sup.optimize_supervised_gpu(
+        torch.from_numpy(coh.packed()), torch.from_numpy(P.copy()), torch.from_numpy(Q.copy()), y,
+        HP["lr"], HP["beta1"], HP["beta2"], HP["reg_adam"], 40, 1, M, HP["lr_decay"],
+        HP["min_lr"], HP["patience"], -1e30, dev, 8192, 1)
+    Pb, Qb = sup.optimize_supervised_original(G, P.copy(), Q.copy(), y, 10000, K, M, N, 0.1, 3, 3)
+    np.savez_compressed(OUT / "supervised.npz", packed=coh.packed(), G=G, y=y, P0=P, P0_packed=P_packed, Q0=Q,
+                        adamem_P=Pa.numpy(), adamem_Q=Qa.numpy(), adamem40_P=P40.numpy(), adamem40_Q=Q40.numpy(),
+                        brqn_P=Pb, brqn_Q=Qb)
+    print("supervised.npz")
+
+
 def align():
     """The reference's cluster alignment across K (plot.py align_clusters_clumppling) on
     seeded Q matrices of equal, larger and smaller K."""
@@ -281,8 +318,8 @@ def align():
 
 
 if __name__ == "__main__":
-    which = set(sys.argv[1:]) or {"edge", "synth", "demo", "demo_gpu", "solvers", "cv_proj", "align"}
-    if which & {"edge", "synth", "demo", "cv_proj"}:
+    which = set(sys.argv[1:]) or {"edge", "synth", "demo", "demo_gpu", "solvers", "cv_proj", "align", "supervised"}
+    if which & {"edge", "synth", "demo", "cv_proj", "supervised"}:
         em, utils = reference()
         if "edge" in which:
             edge(em, utils)
@@ -292,6 +329,8 @@ if __name__ == "__main__":
             demo(em, utils)
         if "cv_proj" in which:
             cv_proj(em, utils)
+        if "supervised" in which:
+            supervised(em, utils)
     if "demo_gpu" in which:
         demo_gpu()
     if "solvers" in which:
