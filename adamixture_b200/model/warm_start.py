@@ -21,7 +21,7 @@ from (P_als, Q0) (this library's E-step and targets); the alternative ``m_step_P
 the membership-weighted allele frequencies ``P_jk = sum_i g_ji Q_ik / (2 sum_i obs_ji
 Q_ik)`` from two products of the packed genotypes (``ops.rsvd_rows``), which measured far
 worse (it discards the ALS P). Plain EM from the ALS start stays the fallback and the
-judge: ``warm_start_fit`` keeps the warm run only if its converged log-likelihood is no
+yardstick: ``warm_start_fit`` keeps the warm run only if its converged log-likelihood is no
 worse than the plain run's (within 1e-6 relative).
 """
 from __future__ import annotations

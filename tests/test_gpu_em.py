@@ -3,7 +3,7 @@
 Bars (written per test):
   * decode / layout / counts / sampler: bit-exact;
   * E-step statistics, float64 mode: rtol 1e-10 against the reference's float64 torch path;
-  * per-iteration P/Q, float64 mode: 1e-5 max abs (the north-star bar; observed ~1e-12);
+  * per-iteration P/Q, float64 mode: 1e-5 max abs (the per-iteration parity bar; observed ~1e-12);
   * per-iteration P/Q, float32 mode: 1e-5 max abs on the 301-sample cohort; on the
     105-sample demo cohort 99.9% of entries within 1e-5 and all within 2e-4 (Adam divides
     each step by sqrt(v), which scales a float32 rounding of a near-zero EM delta by
