@@ -8,7 +8,8 @@
 // integer every packed quad (4 entries: f >= 1e-20, so the product never leaves the normal
 // range). log(prod) + e*ln2 once per thread gives the same sum as the per-entry logs to
 // float64 rounding (each multiply adds <= 2^-53 relative error, i.e. <= 1.1e-16 absolute in
-// the log). h is formed in float64 (ADX_F64) or float32 (ADX_F32) from P and Q of that type.
+// the log). h is formed in float64 (ADX_F64) or float32 (ADX_F32) from P and Q of that type;
+// with a float32 h the factor is formed in float32 too (the running product stays float64).
 // Per-block float64 partials are summed by a one-block kernel in block order: deterministic.
 #include "common.cuh"
 
@@ -20,7 +21,7 @@
 namespace adx {
 
 constexpr int LL_TPB = 256;
-constexpr int LL_BLOCKS = 1184;  // 8 per SM on 148 SMs; fixed so the summation order is
+constexpr int LL_BLOCKS = 1184;  // 8 per SM on 148 SMs; fixed, so the summation order does not depend on the GPU
 
 template <typename R, int KMAX>
 struct LlCfg {
@@ -89,10 +90,20 @@ loglik_kernel(const uint8_t* __restrict__ G, const R* __restrict__ P, const R* _
             R h = 0;
 #pragma unroll
             for (int k = 0; k < KMAX; ++k) h += Ps[jl][k] * q[u][k];
-            const double hd = fmin(fmax((double)h, LL_CLAMP), 1.0 - LL_CLAMP);
-            const double om = 1.0 - hd;
-            const double f = g == 0u ? om * om : (g == 1u ? hd * om : (g == 2u ? hd * hd : 1.0));
-            prod[u] *= f;
+            if constexpr (sizeof(R) == 4) {
+              // float32 h: the factor in float32 as well (its rounding, 6e-8 relative, is below
+              // that of h itself); the clamp h in [1e-10, 1-1e-10] is applied to h and to 1-h,
+              // since 1-1e-10 is not a float32 value; f >= 1e-20 stays a normal float
+              const float hf = fmaxf(h, (float)LL_CLAMP);
+              const float om = fmaxf(1.0f - h, (float)LL_CLAMP);
+              const float f = g == 0u ? om * om : (g == 1u ? hf * om : (g == 2u ? hf * hf : 1.0f));
+              prod[u] *= (double)f;
+            } else {
+              const double hd = fmin(fmax((double)h, LL_CLAMP), 1.0 - LL_CLAMP);
+              const double om = 1.0 - hd;
+              const double f = g == 0u ? om * om : (g == 1u ? hd * om : (g == 2u ? hd * hd : 1.0));
+              prod[u] *= f;
+            }
           }
         }
 #pragma unroll

@@ -438,6 +438,89 @@ def run_e2e(args, G_dev, P0, Q0, M, N, K, prec, dev):
                     "best P/Q copied to the host"}
 
 
+def run_kernels(args, cfg):
+    """Per-kernel timings at the config's shape (CUDA events, mean of ``reps`` launches after
+    one warm-up): the randomized-SVD products, the log-likelihood, BVLS, the BR-QN
+    gradient/Hessian passes and SQP solves, CV masking + deviance, and the warm-start network.
+    One JSON line with achieved GB/s (algorithmic bytes) and GFLOP/s per kernel."""
+    import torch
+
+    from adamixture_b200 import ops
+    from adamixture_b200.model import warm_start as ws
+    from adamixture_b200.src.simulate import make_cohort
+
+    dev = torch.device("cuda", 0)
+    N, M, K = cfg["N"], cfg["M"], cfg["K"]
+    coh = make_cohort(N, M, K, cfg["F"], cfg["alpha"], cfg["miss"], cfg["seed"])
+    G = ops.simulate_packed(torch.from_numpy(coh.Pq.astype(np.int32)).to(dev),
+                            torch.from_numpy(coh.Qq.astype(np.int32)).to(dev), coh.miss_q, coh.keys)
+    rng = np.random.default_rng(1)
+    P = torch.from_numpy(np.clip(rng.random((M, K)), 1e-5, 1 - 1e-5)).to(dev)
+    Q = torch.from_numpy(rng.dirichlet(np.ones(K), N)).to(dev)
+    f = ops.allele_frequency(G, M)
+    hbm, _ = peaks()
+    gbytes = ((M + 3) // 4) * N
+    out = {}
+
+    def timed(name, fn, nbytes=None, flops=None, reps=3):
+        fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / reps
+        r = {"ms": ms}
+        if nbytes:
+            r["GBps"] = nbytes / (ms * 1e-3) / 1e9
+            r["hbm_frac"] = r["GBps"] / hbm
+        if flops:
+            r["GFLOPps"] = flops / (ms * 1e-3) / 1e9
+        out[name] = r
+
+    L = 20
+    B = torch.randn((N, L), device=dev)
+    Y = torch.randn((M, L), device=dev)
+    timed("rsvd_rows_L20", lambda: ops.rsvd_rows(G, f, B, M), gbytes + 4 * L * (M + N), 2.0 * M * N * L)
+    timed("rsvd_cols_L20", lambda: ops.rsvd_cols(G, f, Y, M), gbytes + 4 * L * (M + N), 2.0 * M * N * L)
+    timed("loglik_f64", lambda: ops.loglik_device(G, P, Q, M, "f64"), gbytes + 8 * K * (M + N), 4.0 * M * N * K)
+    P32, Q32 = P.float().contiguous(), Q.float().contiguous()
+    timed("loglik_f32", lambda: ops.loglik_device(G, P32, Q32, M, "f32"), gbytes + 4 * K * (M + N), 4.0 * M * N * K)
+    A = (Q.T @ Q).contiguous()
+    Bt = (P @ A).contiguous()
+    timed("bvls_M_rows", lambda: ops.bvls(A, Bt, 0.0, 1.0), 16 * M * K)
+    v_kk = torch.linalg.svd(torch.ones((1, K), dtype=torch.float64), full_matrices=True)[2].t().contiguous().to(dev)
+    if not args.kernels_skip_hessian:
+        XtX_q, Xtz_q = ops.grad_hess_q(G, P, Q, M)
+        XtX_p, Xtz_p = ops.grad_hess_p(G, P, Q, M)
+        timed("grad_hess_q", lambda: ops.grad_hess_q(G, P, Q, M, XtX_q, Xtz_q), gbytes + 8 * N * K * (K + 1),
+              2.0 * M * N * K * (K + 1), reps=1)
+        timed("grad_hess_p", lambda: ops.grad_hess_p(G, P, Q, M, XtX_p, Xtz_p), gbytes + 8 * M * K * (K + 1),
+              1.0 * M * N * K * (K + 1), reps=1)
+        Xn = (-Xtz_q).contiguous()
+        timed("sqp_q_N_rows", lambda: ops.sqp_solve_q(XtX_q, Xn, Q, v_kk, N, K), 8 * N * K * (K + 2))
+        Xp = (-Xtz_p).contiguous()
+        timed("sqp_p_M_rows", lambda: ops.sqp_solve_p(XtX_p, Xp, P, M, K), 8 * M * K * (K + 2))
+        del XtX_q, XtX_p
+    Gm = ops.masked_copy(G)
+    timed("cv_mask_hash", lambda: ops.cv_mask_hash(Gm, G, M, 42, 5, 0), 2 * gbytes)
+    timed("cv_deviance_hash", lambda: ops.cv_deviance_hash(G, P, Q, M, 42, 5, 0), gbytes + 8 * K * (M + N))
+    del Gm
+    net = ws.WarmStartMLP(dev)
+    X = torch.randn((N, ws.D_IN), device=dev)
+    prior = torch.zeros((N, ws.KMAX), device=dev)
+    T = torch.full((N, ws.KMAX), 1.0 / ws.KMAX, device=dev)
+    fwd_flops = 2.0 * N * (ws.D_IN * ws.H + ws.H * ws.H + ws.H * ws.KMAX)
+    timed("mlp_forward", lambda: net.forward(X, prior), None, fwd_flops)
+    timed("mlp_forward_backward", lambda: net.gradients(X, prior, T), None, 3 * fwd_flops)
+    line = {"metric": "kernel timings", "config": {"workload": cfg["workload"], "N": N, "M": M, "K": K,
+            "note": "CUDA events, mean of 3 launches after one warm-up (Hessian passes: 1); GBps from "
+                    "algorithmic bytes, hbm_frac against the measured copy bandwidth"}, "kernels": out}
+    print(json.dumps(line), flush=True)
+
+
 def run_converge(args, cfg):
     """Time to the converged log-likelihood at the config: from the reference's default
     start (randomized SVD + ALS), plain float32 Adam-EM to its stop, then BF16, mixed
@@ -553,6 +636,8 @@ def main():
     ap.add_argument("--converge", action="store_true",
                     help="instead of the throughput line, time runs to the converged log-likelihood")
     ap.add_argument("--converge-max-iter", dest="converge_max_iter", type=int, default=300)
+    ap.add_argument("--kernels", action="store_true", help="per-kernel timings at the config's shape")
+    ap.add_argument("--kernels-skip-hessian", dest="kernels_skip_hessian", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:
         print("bench.py: --warmup must be >= 3", file=sys.stderr)
@@ -567,6 +652,10 @@ def main():
     if args.converge:
         if rank == 0:
             run_converge(args, cfg)
+        return
+    if args.kernels:
+        if rank == 0:
+            run_kernels(args, cfg)
         return
     run_gpu_arm(args, cfg, rank, world, local_rank)
 
