@@ -11,24 +11,25 @@
 // coefficient matrices per 8192-SNP chunk and contracts them with einsum); the per-entry
 // arithmetic follows adamixture/src/utils_c/cython/sqp.pyx:258-328.
 //
-// One kernel serves both sides: a CTA owns a tile of 32 "rows" (samples for Q, SNPs for
-// P) and a block of up to 128 (k <= l) pairs of the symmetric K x K Hessian, and reduces
-// over a range of the other axis in chunks of 32. Per chunk the CTA computes h and the
-// coefficients of the 32 x 32 entries once into shared memory, then each thread (row r =
-// lane, pair slot = warp) accumulates 16 pairs in registers. Ranges of the reduced axis
-// are split across CTAs when the row tiles alone do not fill the GPU; their sums meet in
-// float64 atomics on the zeroed outputs.
+// Each pass is a GEMM with a fused prologue. The Hessian of a row (sample for Q, SNP for P)
+// is a weighted sum over the other axis of per-entry pair products -- P_jk P_jl (and the
+// complement's) for the Q side, Q_ik Q_il for the P side -- and those products do not depend
+// on the row. A CTA owns 64 rows and 64 (k <= l) pairs of the symmetric K x K Hessian and
+// walks a range of the other axis in chunks of 32: per chunk it stages the factor rows,
+// forms the 32 x 64 pair products and the 64 x 32 coefficients (h, then a/h and b/(1-h))
+// once in shared memory, and each thread accumulates a 4-row x 4-pair tile of the product
+// (register-tiled float64 FMAs). The gradient rides along in the CTAs of the first pair
+// block. Ranges of the reduced axis are split across CTAs when the row tiles alone do not
+// fill the GPU; their sums meet in float64 atomics on the zeroed outputs.
 #include "common.cuh"
 
 namespace adx {
 namespace gh {
 
-constexpr int TR = 32;       // rows per tile
+constexpr int TR = 64;       // rows per tile
+constexpr int TP = 64;       // pairs per tile
 constexpr int CJ = 32;       // reduced-axis entries per chunk
-constexpr int SLOTS = 8;     // warps
-constexpr int PER_T = 16;    // pairs per thread
-constexpr int PAIRS = SLOTS * PER_T;  // pairs per CTA
-constexpr int TPB = 32 * SLOTS;
+constexpr int TPB = 256;     // 16 row groups x 16 pair groups, 4 x 4 each
 
 struct Args {
   const uint8_t* G;
@@ -43,20 +44,33 @@ struct Args {
   int64_t chunks_per_split;
 };
 
+// shared-memory layout (doubles unless noted)
+struct Smem {
+  double *own, *fac, *coef, *zc, *pp;
+  uint8_t *pk, *pl;
+  static __host__ size_t bytes(int K, int nt) {
+    return sizeof(double) * ((size_t)(TR + CJ) * K + (size_t)nt * CJ * TR * 2 + (size_t)nt * CJ * TP) + 2 * TP;
+  }
+  __device__ Smem(uint8_t* base, int K, int nt) {
+    double* d = reinterpret_cast<double*>(base);
+    own = d; d += TR * K;            // [TR][K] factors of the tile's rows
+    fac = d; d += CJ * K;            // [CJ][K] factors of the chunk's reduced entries
+    coef = d; d += nt * CJ * TR;     // [nt][CJ][TR] Hessian coefficients
+    zc = d; d += nt * CJ * TR;       // [nt][CJ][TR] gradient coefficients
+    pp = d; d += nt * CJ * TP;       // [nt][CJ][TP] pair products
+    pk = reinterpret_cast<uint8_t*>(d);
+    pl = pk + TP;
+  }
+};
+
 template <bool QSIDE>
 __global__ void __launch_bounds__(TPB) grad_hess_kernel(Args a) {
+  constexpr int NT = QSIDE ? 2 : 1;   // coefficient terms
   extern __shared__ __align__(16) uint8_t smem[];
   const int K = a.K;
-  double* own = reinterpret_cast<double*>(smem);          // [TR][K]  rows' factors
-  double* fac = own + TR * K;                             // [CJ][K]  reduced-axis factors
-  double* c1 = fac + CJ * K;                              // [CJ][TR] coefficient planes
-  double* c2 = c1 + CJ * TR;
-  double* d1 = c2 + CJ * TR;
-  double* d2 = d1 + CJ * TR;
-  uint8_t* pk = reinterpret_cast<uint8_t*>(d2 + CJ * TR); // pair table (k, l)
-  uint8_t* pl = pk + PAIRS;
-
-  const int tid = threadIdx.x, lane = tid & 31, slot = tid >> 5;
+  Smem s(smem, K, NT);
+  const int tid = threadIdx.x;
+  const int rg = tid & 15, pg = tid >> 4;   // row group, pair group
   const int64_t n_rows = QSIDE ? a.N : a.M;
   const int64_t n_red = QSIDE ? a.M : a.N;
   const double* ownF = QSIDE ? a.Q : a.P;
@@ -67,113 +81,153 @@ __global__ void __launch_bounds__(TPB) grad_hess_kernel(Args a) {
   const int split = (int)(b % a.n_split); b /= a.n_split;
   const int64_t row0 = b * TR;
   const int n_pairs = K * (K + 1) / 2;
+  const bool do_grad = pblk == 0;
 
-  // pair table: pairs pblk*PAIRS + t in row-major order of the upper triangle
-  for (int t = tid; t < PAIRS; t += TPB) {
-    int p = pblk * PAIRS + t, k = 0;
+  // pair table: pairs pblk*TP + t in row-major order of the upper triangle
+  for (int t = tid; t < TP; t += TPB) {
+    int p = pblk * TP + t, k = 0;
     if (p < n_pairs) {
       while (p >= K - k) { p -= K - k; ++k; }
-      pk[t] = (uint8_t)k;
-      pl[t] = (uint8_t)(k + p);
+      s.pk[t] = (uint8_t)k;
+      s.pl[t] = (uint8_t)(k + p);
     } else {
-      pk[t] = 0xFF;
-      pl[t] = 0xFF;
+      s.pk[t] = 0xFF;
+      s.pl[t] = 0xFF;
     }
   }
   for (int e = tid; e < TR * K; e += TPB) {
     const int r = e / K, k = e - r * K;
     const int64_t row = row0 + r;
-    own[e] = row < n_rows ? ownF[row * K + k] : 0.0;
+    s.own[e] = row < n_rows ? ownF[row * K + k] : 0.0;
   }
 
-  double acc[PER_T], xz[8];
+  double acc[4][4];
 #pragma unroll
-  for (int q = 0; q < PER_T; ++q) acc[q] = 0.0;
+  for (int i = 0; i < 4; ++i)
 #pragma unroll
-  for (int m = 0; m < 8; ++m) xz[m] = 0.0;
+    for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
+  // gradient: thread (row r = tid & 63, k = (tid >> 6) + 4 m), m < 16
+  double xz[16];
+#pragma unroll
+  for (int m = 0; m < 16; ++m) xz[m] = 0.0;
+  const int gr = tid & (TR - 1), gk0 = tid >> 6;
 
   const int64_t n_chunks = (n_red + CJ - 1) / CJ;
   const int64_t ch0 = (int64_t)split * a.chunks_per_split;
   const int64_t ch1 = min(n_chunks, ch0 + a.chunks_per_split);
   for (int64_t ch = ch0; ch < ch1; ++ch) {
     const int64_t red0 = ch * CJ;
-    __syncthreads();  // previous chunk's readers are done
+    __syncthreads();  // the previous chunk's readers are done
     for (int e = tid; e < CJ * K; e += TPB) {
       const int c = e / K, k = e - c * K;
       const int64_t j = red0 + c;
-      fac[e] = j < n_red ? redF[j * K + k] : 0.0;
+      s.fac[e] = j < n_red ? redF[j * K + k] : 0.0;
     }
     __syncthreads();
+    // pair products of the chunk's entries (shared by every row)
+    for (int e = tid; e < CJ * TP; e += TPB) {
+      const int c = e / TP, t = e - c * TP;
+      const int k = s.pk[t];
+      double v0 = 0.0, v1 = 0.0;
+      if (k != 0xFF) {
+        const int l = s.pl[t];
+        const double fk = s.fac[c * K + k], fl = s.fac[c * K + l];
+        v0 = fk * fl;
+        if (QSIDE) v1 = (1.0 - fk) * (1.0 - fl);
+      }
+      s.pp[c * TP + t] = v0;
+      if (QSIDE) s.pp[CJ * TP + c * TP + t] = v1;
+    }
     // coefficients of the TR x CJ entries; lanes walk the sample axis of G
     for (int e = tid; e < TR * CJ; e += TPB) {
       int r, c;
       if (QSIDE) { c = e / TR; r = e - c * TR; } else { r = e / CJ; c = e - r * CJ; }
       const int64_t row = row0 + r, red = red0 + c;
-      double v1 = 0.0, v2 = 0.0, w1 = 0.0, w2 = 0.0;
+      double w1 = 0.0, w2 = 0.0, z1 = 0.0, z2 = 0.0;
       if (row < n_rows && red < n_red) {
         const int64_t snp = QSIDE ? red : row, smp = QSIDE ? row : red;
         const unsigned g = genotype(a.G[(snp >> 2) * a.N + smp], (int)(snp & 3));
         if (g != 3u) {
           double h = 0.0;
-          for (int k = 0; k < K; ++k) h += own[r * K + k] * fac[c * K + k];
+          for (int k = 0; k < K; ++k) h += s.own[r * K + k] * s.fac[c * K + k];
           h = fmax(fmin(h, 1.0 - 1e-10), 1e-10);
-          const double gd = (double)g;
-          v1 = gd / h;
-          v2 = (2.0 - gd) / (1.0 - h);
-          w1 = v1 / h;
-          w2 = v2 / (1.0 - h);
+          const double gd = (double)g, om = 1.0 - h;
+          // one division: 1/h and 1/(1-h) from 1/(h(1-h))
+          const double rr = 1.0 / (h * om);
+          const double ih = om * rr, iom = h * rr;
+          z1 = gd * ih;
+          z2 = (2.0 - gd) * iom;
+          w1 = z1 * ih;
+          w2 = z2 * iom;
         }
       }
-      c1[c * TR + r] = v1;
-      c2[c * TR + r] = v2;
-      d1[c * TR + r] = w1;
-      d2[c * TR + r] = w2;
+      if (QSIDE) {
+        s.coef[c * TR + r] = w1;
+        s.coef[CJ * TR + c * TR + r] = w2;
+        s.zc[c * TR + r] = z1;
+        s.zc[CJ * TR + c * TR + r] = z2;
+      } else {
+        s.coef[c * TR + r] = w1 + w2;
+        s.zc[c * TR + r] = z1 - z2;
+      }
     }
     __syncthreads();
     const int cmax = (int)min((int64_t)CJ, n_red - red0);
-    for (int c = 0; c < cmax; ++c) {
-      const double* f = fac + c * K;
-      const double e1 = d1[c * TR + lane], e2 = d2[c * TR + lane];
 #pragma unroll
-      for (int q = 0; q < PER_T; ++q) {
-        const int t = slot + SLOTS * q;
-        const int k = pk[t];
-        if (k == 0xFF) continue;
-        const int l = pl[t];
-        if (QSIDE) {
-          acc[q] += e1 * f[k] * f[l] + e2 * (1.0 - f[k]) * (1.0 - f[l]);
-        } else {
-          acc[q] += (e1 + e2) * f[k] * f[l];
-        }
+    for (int t = 0; t < NT; ++t) {
+      const double* cf = s.coef + t * CJ * TR + rg * 4;
+      const double* pr = s.pp + t * CJ * TP + pg * 4;
+      for (int c = 0; c < cmax; ++c) {
+        const double2 a01 = *reinterpret_cast<const double2*>(cf + c * TR);
+        const double2 a23 = *reinterpret_cast<const double2*>(cf + c * TR + 2);
+        const double2 b01 = *reinterpret_cast<const double2*>(pr + c * TP);
+        const double2 b23 = *reinterpret_cast<const double2*>(pr + c * TP + 2);
+        const double av[4] = {a01.x, a01.y, a23.x, a23.y};
+        const double bv[4] = {b01.x, b01.y, b23.x, b23.y};
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+          for (int j = 0; j < 4; ++j) acc[i][j] = fma(av[i], bv[j], acc[i][j]);
       }
-      if (pblk == 0) {
-        const double z1 = c1[c * TR + lane], z2 = c2[c * TR + lane];
+    }
+    if (do_grad) {
+      for (int c = 0; c < cmax; ++c) {
+        const double* f = s.fac + c * K;
+        const double y1 = s.zc[c * TR + gr];
+        const double y2 = QSIDE ? s.zc[CJ * TR + c * TR + gr] : 0.0;
 #pragma unroll
-        for (int m = 0; m < 8; ++m) {
-          const int k = slot + SLOTS * m;
-          if (k < K) xz[m] += QSIDE ? (z1 * f[k] + z2 * (1.0 - f[k])) : ((z1 - z2) * f[k]);
+        for (int m = 0; m < 16; ++m) {
+          const int k = gk0 + 4 * m;
+          if (k < K) xz[m] += QSIDE ? (y1 * f[k] + y2 * (1.0 - f[k])) : (y1 * f[k]);
         }
       }
     }
   }
 
-  const int64_t row = row0 + lane;
-  if (row >= n_rows) return;
-  double* H = a.XtX + row * K * K;
+  // scatter: both halves of the symmetric Hessian
 #pragma unroll
-  for (int q = 0; q < PER_T; ++q) {
-    const int t = slot + SLOTS * q;
-    const int k = pk[t];
-    if (k == 0xFF) continue;
-    const int l = pl[t];
-    atomicAdd(H + k * K + l, acc[q]);
-    if (l != k) atomicAdd(H + l * K + k, acc[q]);
+  for (int i = 0; i < 4; ++i) {
+    const int64_t row = row0 + rg * 4 + i;
+    if (row >= n_rows) continue;
+    double* H = a.XtX + row * K * K;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int t = pg * 4 + j;
+      const int k = s.pk[t];
+      if (k == 0xFF) continue;
+      const int l = s.pl[t];
+      atomicAdd(H + k * K + l, acc[i][j]);
+      if (l != k) atomicAdd(H + l * K + k, acc[i][j]);
+    }
   }
-  if (pblk == 0) {
+  if (do_grad) {
+    const int64_t row = row0 + gr;
+    if (row < n_rows) {
 #pragma unroll
-    for (int m = 0; m < 8; ++m) {
-      const int k = slot + SLOTS * m;
-      if (k < K) atomicAdd(a.Xtz + row * K + k, xz[m]);
+      for (int m = 0; m < 16; ++m) {
+        const int k = gk0 + 4 * m;
+        if (k < K) atomicAdd(a.Xtz + row * K + k, xz[m]);
+      }
     }
   }
 }
@@ -196,7 +250,7 @@ static int grad_hess(const uint8_t* G, int64_t M, int64_t N, int K, const double
   ADX_CUDA_TRY(cudaMemsetAsync(Xtz, 0, (size_t)n_rows * K * sizeof(double), st));
   gh::Args a{G, P, Q, M, N, K, XtX, Xtz, 0, 0, 0};
   const int n_pairs = K * (K + 1) / 2;
-  a.n_pblk = (n_pairs + gh::PAIRS - 1) / gh::PAIRS;
+  a.n_pblk = (n_pairs + gh::TP - 1) / gh::TP;
   const int64_t tiles = ceil_div(n_rows, gh::TR);
   const int64_t n_chunks = ceil_div(n_red, gh::CJ);
   // about 8 CTAs per SM in all
@@ -204,8 +258,7 @@ static int grad_hess(const uint8_t* G, int64_t M, int64_t N, int K, const double
   split = split < 1 ? 1 : (split > n_chunks ? n_chunks : split);
   a.chunks_per_split = ceil_div(n_chunks, split);
   a.n_split = (int)ceil_div(n_chunks, a.chunks_per_split);
-  const size_t smem = (size_t)(gh::TR + gh::CJ) * K * sizeof(double) + 4 * gh::CJ * gh::TR * sizeof(double) +
-                      2 * gh::PAIRS;
+  const size_t smem = gh::Smem::bytes(K, QSIDE ? 2 : 1);
   ADX_CUDA_TRY(cudaFuncSetAttribute(gh::grad_hess_kernel<QSIDE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   const int64_t blocks = tiles * a.n_pblk * a.n_split;
   gh::grad_hess_kernel<QSIDE><<<(unsigned)blocks, gh::TPB, smem, st>>>(a);
