@@ -32,8 +32,11 @@ def read_data(data_path: str, packed: bool = True, chunk_size: int = 8192, chrom
     return unpack(G.cpu().numpy(), M), N, M
 
 
-def write_outputs(Q: np.ndarray, run_name: str, K: int, out_path: str | Path, P: np.ndarray = None) -> None:
-    """``{run_name}.{K}.Q`` (and ``.P``): the reference's text format, written natively."""
+def write_outputs(Q: np.ndarray, run_name: str, K: int, out_path: str | Path, P: np.ndarray = None,
+                  decimals: int | None = None) -> None:
+    """``{run_name}.{K}.Q`` (and ``.P``): the reference's text format, written natively --
+    "%.18e" values (adamixture/src/utils.py:252-273), or "%.{decimals}f" values as the
+    projection and supervised commands write them (``decimals=6``)."""
     out_path = Path(out_path)
     for X, ext in ((Q, "Q"), (P, "P")):
         if X is None:
@@ -41,6 +44,9 @@ def write_outputs(Q: np.ndarray, run_name: str, K: int, out_path: str | Path, P:
         X = np.ascontiguousarray(X.detach().cpu().numpy() if isinstance(X, torch.Tensor) else X, dtype=np.float64)
         if X.ndim == 1:
             X = X[:, None]
-        _lib.call("adx_write_text_matrix", str(out_path / f"{run_name}.{K}.{ext}").encode(), X.ctypes.data,
-                  X.shape[0], X.shape[1], 0)
+        fn = str(out_path / f"{run_name}.{K}.{ext}").encode()
+        if decimals is None:
+            _lib.call("adx_write_text_matrix", fn, X.ctypes.data, X.shape[0], X.shape[1], 0)
+        else:
+            _lib.call("adx_write_text_matrix_fixed", fn, X.ctypes.data, X.shape[0], X.shape[1], decimals, 0)
     log.info("    Q and P matrices saved." if P is not None else "    Q matrix saved.")

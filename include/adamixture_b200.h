@@ -229,6 +229,12 @@ int adx_cv_deviance_hash(const uint8_t* G0, int64_t M, int64_t N, int K, const d
  * all hardware threads. */
 int adx_write_text_matrix(const char* path, const double* X, int64_t rows, int64_t cols,
                           int threads);
+/* The same with "%.<decimals>f" values (0 <= decimals <= 60): byte for byte
+ * np.savetxt(path, X, delimiter=' ', fmt='%.6f') at decimals = 6, the writer of the
+ * projection and supervised commands (adamixture/project_entry.py:289,
+ * adamixture/supervised_entry.py:386-389). */
+int adx_write_text_matrix_fixed(const char* path, const double* X, int64_t rows, int64_t cols,
+                                int decimals, int threads);
 
 /* ---------------------------------------------------------------- warm-start network
  * No counterpart in the reference (a new component of this build). A per-sample network

@@ -77,3 +77,76 @@ def test_bed_decode_leaves_the_estep_status_word_alone(cuda, synth):
     rows = torch.from_numpy(rng.integers(0, 256, size=(M, (N + 3) // 4), dtype=np.uint8)).cuda()
     ops.bed_to_packed(rows, N, M)
     assert ops.em_status(ws, M, N, K, "bf16") == 0
+
+
+def test_project_command_matches_reference(cv_proj, tmp_path):
+    """The projection command end to end (BED in, .P text in, "%.6f" .Q out) against the
+    reference's own Adam-EM and SQP + ZAL projections of the same cohort from the same
+    start (tests/golden/cv_proj.npz; seed 42 draws that start, as the command does)."""
+    import re
+
+    from adamixture_b200 import project_entry
+
+    write_bed(tmp_path / "t", cv_proj["G"])
+    np.savetxt(tmp_path / "ref.3.P", cv_proj["P"], delimiter=" ")
+    for alg, key, tol in (("adamem", "proj_adamem_Q", 1e-5), ("brqn", "proj_brqn_Q", 1e-4)):
+        assert project_entry.main(["--data_path", str(tmp_path / "t.bed"), "--p_path", str(tmp_path / "ref.3.P"),
+                                   "--save_dir", str(tmp_path / "out"), "--name", alg, "--algorithm", alg,
+                                   "--precision", "f64"]) == 0
+        text = (tmp_path / "out" / f"{alg}.3.Q").read_text()
+        assert re.fullmatch(r"(\d\.\d{6} \d\.\d{6} \d\.\d{6}\n)+", text)
+        Q = np.loadtxt(tmp_path / "out" / f"{alg}.3.Q")
+        np.testing.assert_allclose(Q, cv_proj[key], atol=tol + 5e-7)
+    # an SNP count that does not match P's rows is an error, as in the reference
+    np.savetxt(tmp_path / "short.3.P", cv_proj["P"][:-1], delimiter=" ")
+    assert project_entry.main(["--data_path", str(tmp_path / "t.bed"), "--p_path", str(tmp_path / "short.3.P"),
+                               "--save_dir", str(tmp_path / "out"), "--name", "x"]) == 1
+
+
+@pytest.mark.parametrize("alg", ["brqn", "adamem"])
+def test_supervised_command(supervised_golden, tmp_path, alg):
+    """The supervised command end to end: population names (level 2 here) numbered by first
+    appearance, the result equal to the Python API's on the same inputs, the labelled rows
+    snapped, and the log-likelihood that of the reference's own supervised SQP + ZAL run
+    (tests/golden/supervised.npz), whose populations are numbered differently."""
+    from adamixture_b200 import supervised_entry
+    from adamixture_b200.src import utils
+    from adamixture_b200.src import supervised as sup
+    from oracle import em_oracle as orc
+
+    d = supervised_golden
+    M, K = d["P0"].shape
+    N = d["G"].shape[1]
+    write_bed(tmp_path / "s", d["G"])
+    names = {0: "-", 1: "Yoruba", 2: "Han", 3: "Basque"}
+    (tmp_path / "none.txt").write_text("-\n" * N)
+    (tmp_path / "pops.txt").write_text("".join(names[int(v)] + "\n" for v in d["y"]))
+    args = ["--data_path", str(tmp_path / "s.bed"), "--save_dir", str(tmp_path / "out"), "--name", alg,
+            "--labels", str(tmp_path / "none.txt"), "--labels2", str(tmp_path / "pops.txt"), "--level", "2",
+            "--algorithm", alg, "--precision", "f64"]
+    assert supervised_entry.main(args + (["--no_freqs"] if alg == "adamem" else [])) == 0
+    Q = np.loadtxt(tmp_path / "out" / f"{alg}.3.Q")
+    assert (tmp_path / "out" / f"{alg}.3.P").exists() == (alg == "brqn")
+    y2, ids = supervised_entry.labels_to_y(supervised_entry.parse_labels_file(tmp_path / "pops.txt"))
+    assert sorted(ids.values()) == [1, 2, 3]
+    # the Python API on the same inputs
+    G, _, _ = utils.read_data(str(tmp_path / "s.bed"), device=torch.device("cuda"))
+    np.testing.assert_array_equal(G.cpu().numpy(), d["packed"])
+    P0 = sup.init_p_supervised_gpu(G, y2, K, M)
+    Q0 = np.random.default_rng(42).random((N, K))
+    Q0 /= Q0.sum(1, keepdims=True)
+    sup.init_q_supervised(Q0, y2, K)
+    Q0 = torch.from_numpy(Q0).cuda()
+    if alg == "brqn":
+        P2, Q2 = sup.optimize_supervised_original_gpu(G, P0, Q0, y2, 10000, K, M, N, 0.1, 3, 3, G.device, 4096, 0)
+        np.testing.assert_allclose(np.loadtxt(tmp_path / "out" / f"{alg}.3.P"), P2.cpu().numpy(), atol=5e-7 + 1e-12)
+    else:
+        P2, Q2 = sup.optimize_supervised_gpu(G, P0, Q0, y2, 0.005, 0.80, 0.88, 1e-8, 10000, 5, M, 0.5, 1e-4, 3,
+                                             0.1, G.device, 4096, 0, precision="f64")
+    P2, Q2 = P2.cpu().numpy(), Q2.cpu().numpy()
+    np.testing.assert_allclose(Q, Q2, atol=5e-7 + 1e-12)
+    lab = np.flatnonzero(y2 > 0)
+    np.testing.assert_allclose(Q2[lab, y2[lab] - 1], 1 - 1e-5, atol=1e-12)
+    L, Lr = orc.loglik(d["G"], P2, Q2), orc.loglik(d["G"], d["brqn_P"], d["brqn_Q"])
+    print(alg, "supervised command loglik", L, "reference", Lr)
+    assert abs(L - Lr) <= 1e-4 * abs(Lr)
