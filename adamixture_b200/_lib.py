@@ -14,7 +14,7 @@ from pathlib import Path
 LIB_PATH = Path(__file__).resolve().parent / "_lib" / "libadamixture_b200.so"
 
 ADX_OK, ADX_ERR_ARG, ADX_ERR_CUDA, ADX_ERR_WORKSPACE, ADX_ERR_UNSUPPORTED, ADX_ERR_TIMEOUT = 0, 1, 2, 3, 4, 5
-ADX_F64, ADX_F32, ADX_BF16 = 0, 1, 2
+ADX_F64, ADX_F32, ADX_BF16, ADX_F16 = 0, 1, 2, 3
 MAX_K = 64
 
 P = c_void_p

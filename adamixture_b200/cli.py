@@ -4,7 +4,7 @@
     python -m adamixture_b200 --k 8 --data_path cohort.bed --save_dir out --name run --device gpu
 
 Options of the reference that concern other devices or the plotting stack are accepted;
-``--precision`` (f64 | f32 | bf16 | mixed | auto) selects the Adam-EM E-step arithmetic.
+``--precision`` (f64 | f32 | bf16 | f16 | mixed | auto) selects the Adam-EM E-step arithmetic.
 """
 from __future__ import annotations
 
@@ -40,7 +40,7 @@ def add_run_options(p: argparse.ArgumentParser) -> None:
     p.add_argument("--labels3")
     p.add_argument("--colors")
     p.add_argument("--plot", nargs="*")
-    p.add_argument("--precision", choices=["f64", "f32", "bf16", "mixed", "auto"], default=None,
+    p.add_argument("--precision", choices=["f64", "f32", "bf16", "f16", "mixed", "auto"], default=None,
                    help="Adam-EM E-step arithmetic (default: auto)")
 
 
@@ -107,7 +107,7 @@ def parse_args(argv: list[str]) -> argparse.Namespace:
     p.add_argument("--labels2")
     p.add_argument("--labels3")
     p.add_argument("--colors")
-    p.add_argument("--precision", choices=["f64", "f32", "bf16", "mixed", "auto"], default=None)
+    p.add_argument("--precision", choices=["f64", "f32", "bf16", "f16", "mixed", "auto"], default=None)
     a = p.parse_args(argv)
     if a.device != "gpu":
         p.error("this build runs on the GPU only (--device gpu)")

@@ -351,14 +351,14 @@ int tc_plan(int64_t M, int64_t N, int K, int64_t& n_stile, int& n_split, int& n_
 size_t tc_q_bytes(int64_t n_stile);
 int tc_sweep(const uint8_t* G, const float* P, const float* Q, int64_t M, int64_t N, int K,
              int64_t n_stile, int n_split, int n_mblk, float* ABp, float* Tp, void* Qb, int* err,
-             cudaStream_t st);
+             bool f16, cudaStream_t st);
 
 int em_plan(int64_t M, int64_t N, int K, int prec, EmPlan& pl) {
   if (M <= 0 || N <= 0 || K < 1 || K > ADX_MAX_K) return ADX_ERR_ARG;
-  if (prec != ADX_F64 && prec != ADX_F32 && prec != ADX_BF16) return ADX_ERR_UNSUPPORTED;
+  if (prec != ADX_F64 && prec != ADX_F32 && prec != ADX_BF16 && prec != ADX_F16) return ADX_ERR_UNSUPPORTED;
   pl.M = M; pl.N = N; pl.K = K; pl.prec = prec;
   pl.kmax = pick_kmax(K);
-  if (prec == ADX_BF16) {
+  if (prec == ADX_BF16 || prec == ADX_F16) {
     // tensor-core sweep: 896-SNP blocks x 128-sample tiles, float partials
     int64_t n_stile = 0;
     int n_split = 0, n_mblk = 0;
@@ -436,12 +436,12 @@ static int launch_update(const EmPlan& pl, void* ws, int mode, double* A, double
 
 int em_sweep(const EmPlan& pl, const uint8_t* G, const void* P, const void* Q, void* ws,
              cudaStream_t st) {
-  if (pl.prec == ADX_BF16) {
+  if (pl.prec == ADX_BF16 || pl.prec == ADX_F16) {
     float* ABp = reinterpret_cast<float*>(reinterpret_cast<uint8_t*>(ws) + EmPlan::HEADER);
     int* err = reinterpret_cast<int*>(ws);
     void* Qb = reinterpret_cast<uint8_t*>(ws) + pl.extra_offset();
     return tc_sweep(G, (const float*)P, (const float*)Q, pl.M, pl.N, pl.K, pl.n_stile, pl.n_split,
-                    pl.n_mblk, ABp, ABp + pl.ab_elems, Qb, err, st);
+                    pl.n_mblk, ABp, ABp + pl.ab_elems, Qb, err, pl.prec == ADX_F16, st);
   }
   return pl.prec == ADX_F64 ? launch_sweep<double>(pl, G, P, Q, ws, st)
                             : launch_sweep<float>(pl, G, P, Q, ws, st);

@@ -1,6 +1,15 @@
-// Tensor-core (tcgen05, sm_100a) form of the E-step sweep: BF16 operands, FP32 accumulation
-// in tensor memory. Same statistics and the same partial-sum layout as em_sweep_kernel
-// (adamixture/model/em_adam_gpu.py:46-78), for 1 <= K <= 16 (K padded to 16 in the MMAs).
+// Tensor-core (tcgen05, sm_100a) form of the E-step sweep: BF16 or FP16 operands, FP32
+// accumulation in tensor memory. Same statistics and the same partial-sum layout as
+// em_sweep_kernel (adamixture/model/em_adam_gpu.py:46-78), for 1 <= K <= 16 (K padded to 16
+// in the MMAs).
+//
+// Operand formats (one kind::f16 MMA takes both operands in the same format):
+//   BF16: 8-bit significand, values as they are.
+//   FP16: 11-bit significand (8x finer rounding at the same MMA rate), with power-of-two
+//         scalings that keep every operand in FP16's normal range: P, 1-P and Q are stored
+//         x16 (values >= 1e-5 become >= 1.6e-4; the smallest normal is 6.1e-5), a and b x1/4
+//         (at most 2/1e-5/4 = 5e4 < 65504). H then holds 256 h and A/B/T accumulate 4x their
+//         value; the ratio step and the partial-sum writes undo both scalings exactly.
 //
 // Per CTA: R = 7 SNP tiles of 128 SNPs (896 SNPs) and a residue class of 128-sample tiles.
 // For each step (sample tile s, SNP tile r), in two half-steps of 64 samples:
@@ -8,7 +17,7 @@
 //   Hc = (1-P_r) . Q_s^T   (the complement, so 1-h stays accurate when h -> 1)  -> TMEM
 //   consumer warps read H/Hc rows from TMEM and form, per entry (one reciprocal each),
 //     a = g / max(h,1e-5),  b = (2-g) / max(1-h,1e-5)   (0 where missing)
-//   as BF16 tiles in shared memory; after both halves
+//   as BF16/FP16 tiles in shared memory; after both halves
 //   A_r += a . Q_s, B_r += b . Q_s   (M=128 SNPs, N=16, K=128 samples; TMEM, all sample tiles)
 //   T   += a^T . P_r + b^T . (1-P_r) (M=128 samples, N=16, K=128 SNPs; TMEM, all SNP tiles)
 // After the R SNP tiles of a sample tile, T (over the CTA's 896 SNPs) goes to the T partials;
@@ -18,7 +27,7 @@
 // step and as many those of the second 64 (each warpgroup a block of WG_COLS samples); the
 // last warp is the producer. Its lane 0 issues every MMA from precomputed shared-memory
 // descriptors (a step's 34 MMAs cost one 64-bit add per operand), and the warp streams the
-// G tiles (a ring of NG stages, NG-1 steps ahead) and the BF16 Q tiles (NQ buffers, one
+// G tiles (a ring of NG stages, NG-1 steps ahead) and the converted Q tiles (NQ buffers, one
 // sample tile ahead) into shared memory with cp.async. H/Hc live in two TMEM buffers (one
 // per half) and the a/b tiles in two shared-memory buffers (one per step parity), so while
 // one half's warpgroups form their ratios the tensor pipe runs the other half's H and the
@@ -92,14 +101,12 @@ constexpr uint32_t WAIT_LIMIT = 1u << 26;  // ~seconds of polling before giving 
 
 // ---------------------------------------------------------------- descriptors
 
-// Instruction descriptor, kind::f16: BF16 A/B, FP32 D, M = 128.
-__host__ __device__ constexpr uint32_t idesc(int N, int a_mn, int b_mn) {
-  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)a_mn << 15) | ((uint32_t)b_mn << 16) |
+// Instruction descriptor, kind::f16: A/B format fmt (0 = FP16, 1 = BF16) for both, FP32 D,
+// M = 128.
+__host__ __device__ constexpr uint32_t idesc(int N, int a_mn, int b_mn, uint32_t fmt) {
+  return (1u << 4) | (fmt << 7) | (fmt << 10) | ((uint32_t)a_mn << 15) | ((uint32_t)b_mn << 16) |
          ((uint32_t)(N >> 3) << 17) | ((uint32_t)(TILE >> 4) << 24);
 }
-constexpr uint32_t ID_H = idesc(HALF, 0, 0);   // A = P (K-major), B = Q half (K-major)
-constexpr uint32_t ID_AB = idesc(KP, 0, 1);    // A = a (K-major), B = Q (MN-major)
-constexpr uint32_t ID_T = idesc(KP, 1, 1);     // A = a^T (MN-major), B = P (MN-major)
 
 // Shared-memory matrix descriptor, no swizzle, Blackwell version bit.
 __device__ __forceinline__ uint64_t sdesc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
@@ -123,8 +130,8 @@ __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return (uint32_t)__cvta_generic_to_shared(p);
 }
 
-__device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t ad, uint64_t bd, uint32_t id,
-                                         uint32_t accumulate) {
+__device__ __forceinline__ void mma_f16kind(uint32_t tmem_d, uint64_t ad, uint64_t bd, uint32_t id,
+                                            uint32_t accumulate) {
   asm volatile(
       "{\n\t.reg .pred p;\n\t"
       "setp.ne.b32 p, %4, 0;\n\t"
@@ -194,33 +201,61 @@ __device__ __forceinline__ float rcp_approx(float x) {
   asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
   return r;
 }
-__device__ __forceinline__ uint32_t pack_bf16x2(float lo, float hi) {
-  uint32_t r;
-  asm("cvt.rn.bf16x2.f32 %0, %1, %2;" : "=r"(r) : "f"(hi), "f"(lo));
-  return r;
-}
-__device__ __forceinline__ uint32_t mul_bf16x2(uint32_t a, uint32_t b) {
-  uint32_t r;
-  asm("mul.rn.bf16x2 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(b));
-  return r;
-}
 __device__ __forceinline__ uint32_t prmt(uint32_t a, uint32_t b, uint32_t sel) {
   uint32_t r;
   asm("prmt.b32 %0, %1, %2, %3;" : "=r"(r) : "r"(a), "r"(b), "r"(sel));
   return r;
 }
 
-// Genotype weights as BF16 pairs, looked up with one byte permute per pair:
-// entry g (16 bits) at bytes 2g..2g+1 of {hi:lo}.
-constexpr uint32_t GA_LO = 0x3F800000u, GA_HI = 0x00004000u;  // g -> {0, 1, 2, 0}
-constexpr uint32_t GB_LO = 0x3F804000u, GB_HI = 0x00000000u;  // g -> {2, 1, 0, 0}
+// Operand format traits. GA/GB: the genotype weights g -> {0, 1, 2, 0} (a) and
+// g -> {2, 1, 0, 0} (b) as 16-bit pairs, looked up with one byte permute per pair (entry g
+// at bytes 2g..2g+1 of {hi:lo}). PQ_SCALE: factor on stored P, 1-P and Q; H_UNITS: h in
+// H's units (the 1e-5 clamp is applied there); R_SCALE: factor on 1/(h(1-h)) so the stored
+// ratios carry the 1/4 (FP16); OUT_SCALE: factor that takes the accumulated A/B/T back to
+// their values.
+template <bool F16>
+struct Fmt;
+template <>
+struct Fmt<false> {
+  static constexpr uint32_t CODE = 1;  // BF16
+  static constexpr uint32_t GA_LO = 0x3F800000u, GA_HI = 0x00004000u;
+  static constexpr uint32_t GB_LO = 0x3F804000u, GB_HI = 0x00000000u;
+  static constexpr float PQ_SCALE = 1.0f, H_UNITS = 1.0f, R_SCALE = 1.0f, OUT_SCALE = 1.0f;
+  static __device__ __forceinline__ uint32_t pack(float lo, float hi) {
+    uint32_t r;
+    asm("cvt.rn.bf16x2.f32 %0, %1, %2;" : "=r"(r) : "f"(hi), "f"(lo));
+    return r;
+  }
+  static __device__ __forceinline__ uint32_t mul(uint32_t a, uint32_t b) {
+    uint32_t r;
+    asm("mul.rn.bf16x2 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(b));
+    return r;
+  }
+};
+template <>
+struct Fmt<true> {
+  static constexpr uint32_t CODE = 0;  // FP16
+  static constexpr uint32_t GA_LO = 0x3C000000u, GA_HI = 0x00004000u;
+  static constexpr uint32_t GB_LO = 0x3C004000u, GB_HI = 0x00000000u;
+  static constexpr float PQ_SCALE = 16.0f, H_UNITS = 256.0f, R_SCALE = 64.0f, OUT_SCALE = 0.25f;
+  static __device__ __forceinline__ uint32_t pack(float lo, float hi) {
+    uint32_t r;
+    asm("cvt.rn.f16x2.f32 %0, %1, %2;" : "=r"(r) : "f"(hi), "f"(lo));
+    return r;
+  }
+  static __device__ __forceinline__ uint32_t mul(uint32_t a, uint32_t b) {
+    uint32_t r;
+    asm("mul.rn.f16x2 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(b));
+    return r;
+  }
+};
 
 // ---------------------------------------------------------------- kernel
 
 struct Args {
   const uint8_t* G;
   const float* P;     // [M][K] float32
-  const uint8_t* Qb;  // BF16 Q tiles [n_stile][4096 B], shared-memory layout
+  const uint8_t* Qb;  // converted Q tiles [n_stile][4096 B], shared-memory layout
   int64_t M, N;
   int K;
   int64_t n_stile;    // sample tiles
@@ -231,10 +266,13 @@ struct Args {
   int* err;
 };
 
-// Q (float32 [N][K]) -> BF16 tiles of 128 samples x 16 in the shared-memory layout of a Q
-// tile (rows past N and columns past K are zero), so the producer copies them verbatim.
-__global__ void q_to_bf16_kernel(const float* __restrict__ Q, int64_t N, int K, int64_t n_stile,
-                                 uint8_t* __restrict__ Qb) {
+// Q (float32 [N][K]) -> operand-format tiles (x PQ_SCALE) of 128 samples x 16 in the
+// shared-memory layout of a Q tile (rows past N and columns past K are zero), so the
+// producer copies them verbatim.
+template <bool F16>
+__global__ void q_to_tiles_kernel(const float* __restrict__ Q, int64_t N, int K, int64_t n_stile,
+                                  uint8_t* __restrict__ Qb) {
+  using F = Fmt<F16>;
   const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= n_stile * TILE * 2) return;
   const int64_t tile = e / (TILE * 2);
@@ -244,10 +282,10 @@ __global__ void q_to_bf16_kernel(const float* __restrict__ Q, int64_t N, int K, 
 #pragma unroll
   for (int q = 0; q < 8; ++q) {
     const int k = kh + q;
-    f[q] = (i < N && k < K) ? __ldg(Q + i * K + k) : 0.0f;
+    f[q] = (i < N && k < K) ? __ldg(Q + i * K + k) * F::PQ_SCALE : 0.0f;
   }
   *reinterpret_cast<uint4*>(Qb + tile * P_TILE_BYTES + off_pq(row, kh)) =
-      make_uint4(pack_bf16x2(f[0], f[1]), pack_bf16x2(f[2], f[3]), pack_bf16x2(f[4], f[5]), pack_bf16x2(f[6], f[7]));
+      make_uint4(F::pack(f[0], f[1]), F::pack(f[2], f[3]), F::pack(f[4], f[5]), F::pack(f[6], f[7]));
 }
 
 // G tile (32 packed rows x 128 samples) into a shared-memory stage by the producer warp: lane
@@ -280,7 +318,7 @@ __device__ __forceinline__ void producer_load_g(const Args& a, int64_t row0, int
   }
 }
 
-// BF16 Q tile (4096 B) into a shared-memory buffer by the producer warp: lane l copies
+// Converted Q tile (4096 B) into a shared-memory buffer by the producer warp: lane l copies
 // bytes [128 l, 128 l + 128).
 __device__ __forceinline__ void producer_load_q(const Args& a, int64_t tile, uint8_t* qs, uint32_t bar) {
   const int l = threadIdx.x & 31;
@@ -290,7 +328,12 @@ __device__ __forceinline__ void producer_load_q(const Args& a, int64_t tile, uin
   cp_async_arrive(bar);
 }
 
+template <bool F16>
 __global__ void __launch_bounds__(TPB, 1) em_sweep_tc_kernel(Args a) {
+  using F = Fmt<F16>;
+  constexpr uint32_t ID_H = idesc(HALF, 0, 0, F::CODE);   // A = P (K-major), B = Q half (K-major)
+  constexpr uint32_t ID_AB = idesc(KP, 0, 1, F::CODE);    // A = a (K-major), B = Q (MN-major)
+  constexpr uint32_t ID_T = idesc(KP, 1, 1, F::CODE);     // A = a^T (MN-major), B = P (MN-major)
   extern __shared__ uint8_t smem_raw[];
   uint8_t* sm = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   uint32_t* tmem_holder = reinterpret_cast<uint32_t*>(sm + OFF_TMEM);
@@ -335,21 +378,21 @@ __global__ void __launch_bounds__(TPB, 1) em_sweep_tc_kernel(Args a) {
       const int k = kh + q;
       const bool ok = j < a.M && k < a.K;
       const float v = ok ? __ldg(a.P + j * a.K + k) : 0.0f;
-      p[q] = v;
-      c[q] = ok ? 1.0f - v : 0.0f;
+      p[q] = v * F::PQ_SCALE;
+      c[q] = ok ? (1.0f - v) * F::PQ_SCALE : 0.0f;
     }
     uint8_t* pt = sm + OFF_P + r * 2 * P_TILE_BYTES;
     *reinterpret_cast<uint4*>(pt + off_pq(row, kh)) =
-        make_uint4(pack_bf16x2(p[0], p[1]), pack_bf16x2(p[2], p[3]), pack_bf16x2(p[4], p[5]), pack_bf16x2(p[6], p[7]));
+        make_uint4(F::pack(p[0], p[1]), F::pack(p[2], p[3]), F::pack(p[4], p[5]), F::pack(p[6], p[7]));
     *reinterpret_cast<uint4*>(pt + P_TILE_BYTES + off_pq(row, kh)) =
-        make_uint4(pack_bf16x2(c[0], c[1]), pack_bf16x2(c[2], c[3]), pack_bf16x2(c[4], c[5]), pack_bf16x2(c[6], c[7]));
+        make_uint4(F::pack(c[0], c[1]), F::pack(c[2], c[3]), F::pack(c[4], c[5]), F::pack(c[6], c[7]));
   }
   fence_async_smem();
   fence_before();
   __syncthreads();
   fence_after();
   const uint32_t tmem = *tmem_holder;
-  const float ELO = (float)E_CLAMP;
+  const float ELO = (float)E_CLAMP * F::H_UNITS;
 
   // Base descriptors; the offsets added below are in 16-byte units.
   const uint32_t s_p = smem_u32(sm + OFF_P), s_q = smem_u32(sm + OFF_Q), s_a = smem_u32(sm + OFF_A);
@@ -366,8 +409,8 @@ __global__ void __launch_bounds__(TPB, 1) em_sweep_tc_kernel(Args a) {
     const uint64_t bq = dQK + (uint64_t)(qb * 256 + h * 128);
     const uint64_t ap = dPK + (uint64_t)(r * 512);
     const uint32_t col = tmem + (uint32_t)h * 128;
-    mma_bf16(col, ap, bq, ID_H, 0);
-    mma_bf16(col + HALF, ap + 256, bq, ID_H, 0);
+    mma_f16kind(col, ap, bq, ID_H, 0);
+    mma_f16kind(col + HALF, ap + 256, bq, ID_H, 0);
   };
   // A/B/T MMAs of a step on SNP tile r, Q buffer qb, a/b buffer buf
   auto issue_abt = [&](int r, int qb, int buf, bool acc_ab) {
@@ -377,16 +420,16 @@ __global__ void __launch_bounds__(TPB, 1) em_sweep_tc_kernel(Args a) {
 #pragma unroll
     for (int ks = 0; ks < TILE / 16; ++ks) {
       const uint32_t acc = (acc_ab || ks > 0) ? 1u : 0u;
-      mma_bf16(tab, ak + 16 * ks, qm + 32 * ks, ID_AB, acc);
-      mma_bf16(tab + 16, ak + B_OFF + 16 * ks, qm + 32 * ks, ID_AB, acc);
+      mma_f16kind(tab, ak + 16 * ks, qm + 32 * ks, ID_AB, acc);
+      mma_f16kind(tab + 16, ak + B_OFF + 16 * ks, qm + 32 * ks, ID_AB, acc);
     }
     const uint64_t am = dAM + (uint64_t)(buf * 2048);
     const uint64_t pm = dPM + (uint64_t)(r * 512);
 #pragma unroll
     for (int ks = 0; ks < TILE / 16; ++ks) {
       const uint32_t acc = (r > 0 || ks > 0) ? 1u : 0u;
-      mma_bf16(tmem + COL_T, am + 256 * ks, pm + 32 * ks, ID_T, acc);
-      mma_bf16(tmem + COL_T, am + B_OFF + 256 * ks, pm + 256 + 32 * ks, ID_T, 1u);
+      mma_f16kind(tmem + COL_T, am + 256 * ks, pm + 32 * ks, ID_T, acc);
+      mma_f16kind(tmem + COL_T, am + B_OFF + 256 * ks, pm + 256 + 32 * ks, ID_T, 1u);
     }
   };
   auto write_t = [&](int64_t s) {  // one warpgroup: T rows (samples) of sample tile s
@@ -398,7 +441,7 @@ __global__ void __launch_bounds__(TPB, 1) em_sweep_tc_kernel(Args a) {
       float* dst = a.Tp + ((int64_t)mblk * a.N + i) * a.K;
 #pragma unroll
       for (int k = 0; k < KP; ++k)
-        if (k < a.K) dst[k] = __uint_as_float(v[k]);
+        if (k < a.K) dst[k] = __uint_as_float(v[k]) * F::OUT_SCALE;
     }
   };
 
@@ -534,11 +577,12 @@ __global__ void __launch_bounds__(TPB, 1) em_sweep_tc_kernel(Args a) {
             const float rec1 = fmaxf(__uint_as_float(hv[cur][e + 1]), ELO);
             const float omr0 = fmaxf(__uint_as_float(cv[cur][e]), ELO);
             const float omr1 = fmaxf(__uint_as_float(cv[cur][e + 1]), ELO);
-            const float r0 = rcp_approx(rec0 * omr0), r1 = rcp_approx(rec1 * omr1);
-            const uint32_t ypair = pack_bf16x2(omr0 * r0, omr1 * r1);  // 1/rec
-            const uint32_t xpair = pack_bf16x2(rec0 * r0, rec1 * r1);  // 1/(1-rec)
-            ap[e >> 1] = mul_bf16x2(prmt(GA_LO, GA_HI, sel), ypair);
-            bp[e >> 1] = mul_bf16x2(prmt(GB_LO, GB_HI, sel), xpair);
+            float r0 = rcp_approx(rec0 * omr0), r1 = rcp_approx(rec1 * omr1);
+            if constexpr (F16) { r0 *= F::R_SCALE; r1 *= F::R_SCALE; }
+            const uint32_t ypair = F::pack(omr0 * r0, omr1 * r1);  // 1/rec (FP16: 1/(4 rec))
+            const uint32_t xpair = F::pack(rec0 * r0, rec1 * r1);  // 1/(1-rec)
+            ap[e >> 1] = F::mul(prmt(F::GA_LO, F::GA_HI, sel), ypair);
+            bp[e >> 1] = F::mul(prmt(F::GB_LO, F::GB_HI, sel), xpair);
           }
         }
         *reinterpret_cast<uint4*>(ta + off_ab(jl, col0)) = make_uint4(ap[0], ap[1], ap[2], ap[3]);
@@ -585,7 +629,7 @@ __global__ void __launch_bounds__(TPB, 1) em_sweep_tc_kernel(Args a) {
           float* dst = a.ABp + ((int64_t)split * a.M + j) * (2 * a.K) + wg * a.K;
 #pragma unroll
           for (int k = 0; k < KP; ++k)
-            if (k < a.K) dst[k] = __uint_as_float(v[k]);
+            if (k < a.K) dst[k] = __uint_as_float(v[k]) * F::OUT_SCALE;
         }
       }
     }
@@ -613,24 +657,30 @@ int tc_plan(int64_t M, int64_t N, int K, int64_t& n_stile, int& n_split, int& n_
 
 size_t tc_q_bytes(int64_t n_stile) { return (size_t)n_stile * tc::P_TILE_BYTES; }
 
-int tc_sweep(const uint8_t* G, const float* P, const float* Q, int64_t M, int64_t N, int K,
-             int64_t n_stile, int n_split, int n_mblk, float* ABp, float* Tp, void* Qb, int* err,
-             cudaStream_t st) {
+template <bool F16>
+static int tc_launch(const tc::Args& a, int64_t n_stile, uint8_t* qb, const float* Q, cudaStream_t st) {
   static bool attr_set[64] = {false};
   int dev = 0;
   ADX_CUDA_TRY(cudaGetDevice(&dev));
   if (dev >= 0 && dev < 64 && !attr_set[dev]) {
-    ADX_CUDA_TRY(cudaFuncSetAttribute(tc::em_sweep_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    ADX_CUDA_TRY(cudaFuncSetAttribute(tc::em_sweep_tc_kernel<F16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       tc::SMEM_ALLOC));
     attr_set[dev] = true;
   }
-  uint8_t* qb = static_cast<uint8_t*>(Qb);
-  tc::q_to_bf16_kernel<<<(unsigned)ceil_div(n_stile * tc::TILE * 2, 256), 256, 0, st>>>(Q, N, K, n_stile, qb);
+  tc::q_to_tiles_kernel<F16><<<(unsigned)ceil_div(n_stile * tc::TILE * 2, 256), 256, 0, st>>>(Q, a.N, a.K,
+                                                                                                n_stile, qb);
   ADX_LAUNCH_CHECK();
-  tc::Args a{G, P, qb, M, N, K, n_stile, n_split, n_mblk, ABp, Tp, err};
-  tc::em_sweep_tc_kernel<<<(unsigned)(n_split * n_mblk), tc::TPB, tc::SMEM_ALLOC, st>>>(a);
+  tc::em_sweep_tc_kernel<F16><<<(unsigned)(a.n_split * a.n_mblk), tc::TPB, tc::SMEM_ALLOC, st>>>(a);
   ADX_LAUNCH_CHECK();
   return ADX_OK;
+}
+
+int tc_sweep(const uint8_t* G, const float* P, const float* Q, int64_t M, int64_t N, int K,
+             int64_t n_stile, int n_split, int n_mblk, float* ABp, float* Tp, void* Qb, int* err,
+             bool f16, cudaStream_t st) {
+  uint8_t* qb = static_cast<uint8_t*>(Qb);
+  const tc::Args a{G, P, qb, M, N, K, n_stile, n_split, n_mblk, ABp, Tp, err};
+  return f16 ? tc_launch<true>(a, n_stile, qb, Q, st) : tc_launch<false>(a, n_stile, qb, Q, st);
 }
 
 }  // namespace adx

@@ -161,7 +161,7 @@ static int spt_of() { return LlCfg<R, KMAX>::SPT; }
 
 static int ll_plan(int64_t M, int64_t N, int K, int prec, LlPlan& pl) {
   if (M <= 0 || N <= 0 || K < 1 || K > ADX_MAX_K) return ADX_ERR_ARG;
-  if (prec != ADX_F64 && prec != ADX_F32 && prec != ADX_BF16) return ADX_ERR_UNSUPPORTED;
+  if (prec != ADX_F64 && prec != ADX_F32 && prec != ADX_BF16 && prec != ADX_F16) return ADX_ERR_UNSUPPORTED;
   pl.kmax = pick_kmax(K);
   int spt = 1;
 #define S64(KM) spt = spt_of<double, KM>()

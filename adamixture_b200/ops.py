@@ -10,10 +10,10 @@ from __future__ import annotations
 import torch
 
 from . import _lib
-from ._lib import ADX_BF16, ADX_F32, ADX_F64, call, query_size
+from ._lib import ADX_BF16, ADX_F16, ADX_F32, ADX_F64, call, query_size
 
-PRECISIONS = {"f64": ADX_F64, "f32": ADX_F32, "bf16": ADX_BF16}
-_TORCH_OF = {ADX_F64: torch.float64, ADX_F32: torch.float32, ADX_BF16: torch.float32}
+PRECISIONS = {"f64": ADX_F64, "f32": ADX_F32, "bf16": ADX_BF16, "f16": ADX_F16}
+_TORCH_OF = {ADX_F64: torch.float64, ADX_F32: torch.float32, ADX_BF16: torch.float32, ADX_F16: torch.float32}
 
 
 def precision_code(p) -> int:

@@ -2,7 +2,7 @@
 """Benchmark of the ADMIXTURE Adam-EM hot path on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--precision auto|f32|f64|bf16] [--config c3|c2|c1]
+                    [--precision auto|f32|f64|bf16|f16] [--config c3|c2|c1]
 
 Workload (default ``c3``): N=200,000 samples, M=500,000 SNPs, K=10; a seeded synthetic
 admixed cohort (Balding-Nichols F=0.02; Q 70% Dirichlet(0.05) / 30% Dirichlet(1); 1%
@@ -55,6 +55,7 @@ CONFIGS = {
     "c3s": dict(workload="Adam-EM, N=200000 samples, M=50000 SNPs, K=10, F=0.02, Q 0.7*Dir(0.05)+0.3*Dir(1), 1% missing",
                 N=200_000, M=50_000, K=10, F=0.02, alpha=((0.7, 0.05), (0.3, 1.0)), miss=0.01, seed=2000),
 }
+TC_PRECISIONS = ("bf16", "f16")   # the tensor-core sweep
 CHECK = 5
 HP = dict(lr=0.005, beta1=0.80, beta2=0.88, eps=1e-8)
 
@@ -267,7 +268,7 @@ def run_gpu_arm(args, cfg, rank, world, local_rank):
         # kernels per fused iteration: sweep (+ the BF16 copy of Q for the tensor-core sweep)
         # and the update kernel; per check: the log-likelihood kernel and its final sum
         opt = EMAdamOptimizer(P.shape, Q.shape, HP["lr"], HP["beta1"], HP["beta2"], HP["eps"], dev, prec)
-        per_iter = 3 if prec == "bf16" else 2
+        per_iter = 3 if prec in TC_PRECISIONS else 2
 
         def one_step(it):
             opt.fused_iteration(G, P, Q, P32, Q32, M, ws)
@@ -279,7 +280,7 @@ def run_gpu_arm(args, cfg, rank, world, local_rank):
         # SNP-sharded: local sweep + statistics, all-reduce of T, targets, Adam (Q replicated)
         run = ShardedAdamEM(G, P, Q, M_loc, K, HP["beta1"], HP["beta2"], HP["eps"], HP["lr"],
                             backend=CudaBackend(prec))
-        per_iter = (3 if prec == "bf16" else 2) + 2
+        per_iter = (3 if prec in TC_PRECISIONS else 2) + 2
 
         def one_step(it):
             run.iteration()
@@ -333,12 +334,13 @@ def run_gpu_arm(args, cfg, rank, world, local_rank):
     achieved = ab / (sweep_ms * 1e-3) / 1e9
     roof = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
             "frac": achieved / hbm, "traffic": traffic_per_launch(M_loc, N, K, prec),
-            "kernel": "em_sweep_tc_kernel" if prec == "bf16" else f"em_sweep_kernel<{'double' if prec == 'f64' else 'float'},{ops_kmax(K)}>",
+            "kernel": f"em_sweep_tc_kernel<{prec == 'f16'}>" if prec in TC_PRECISIONS else f"em_sweep_kernel<{'double' if prec == 'f64' else 'float'},{ops_kmax(K)}>",
             "launch_ms": sweep_ms, "alg_bytes": ab, "peak_kind": peak_kind,
             "entries_per_s": M_loc * N / (sweep_ms * 1e-3), "snp_rows_per_rank": M_loc}
-    if prec == "bf16":
+    if prec in TC_PRECISIONS:
         # the contractions (h, 1-h, A, B, T: 8 M N K flops of useful work; K padded to 16 in
-        # the MMAs) against the measured dense BF16 peak, for the tensor-core sweep
+        # the MMAs) against the measured dense BF16 peak (FP16's dense rate is the same), for
+        # the tensor-core sweep
         tf = peaks_tensor()
         flops = 8.0 * M_loc * N * K
         roof["tensor"] = {"achieved_tflops": flops / (sweep_ms * 1e-3) / 1e12, "peak_tflops": tf,
@@ -364,7 +366,7 @@ def run_gpu_arm(args, cfg, rank, world, local_rank):
             "metric": METRIC, "value": 1000.0 / ms_per_step, "unit": UNIT,
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "strong",
-            "vs_baseline": None, "dtype": {"f64": "f64", "f32": "f32", "bf16": "bf16"}[prec],
+            "vs_baseline": None, "dtype": {"f64": "f64", "f32": "f32", "bf16": "bf16", "f16": "f16"}[prec],
             "data": "synthetic",
             "config": {"workload": cfg["workload"], "precision": prec, "check_every": CHECK,
                        "l2": "inputs (packed G) larger than L2; no flush",
@@ -563,13 +565,14 @@ def run_converge(args, cfg):
     fit("plain_f32", P0, Q0, "f32")
     target = max(e[1] for e in runs["plain_f32"]["trace"])
     fit("bf16", P0, Q0, "bf16" if 8 <= K <= 16 else "f32")
+    fit("f16", P0, Q0, "f16" if 8 <= K <= 16 else "f32")
     fit("mixed", P0, Q0, "mixed")
     net = ws.WarmStartMLP.load(ws.DEFAULT_WEIGHTS, dev)
     torch.cuda.synchronize()
     t = time.perf_counter()
     Pw, Qw = ws.predict(net, G, M, U, S, V, Q0, P0)
     torch.cuda.synchronize()
-    fit("warm_mixed", Pw, Qw, "mixed", extra_s=time.perf_counter() - t)
+    fit("warm_auto", Pw, Qw, "auto", extra_s=time.perf_counter() - t)
     out = {}
     for name, r in runs.items():
         reach = next(((it, sec) for it, L, sec in r["trace"] if L >= target - 1e-6 * abs(target)), None)

@@ -11,8 +11,9 @@
  *    bits 2*(j&3); 0/1/2 = allele count, 3 = missing; unused bits of the last row are 0.
  *    (The reference's GPU layout, adamixture/src/utils_c/cython/snp_reader.pyx:76-120.)
  *  - P is [M][K], Q is [N][K], row-major. "precision" selects the E-step arithmetic:
- *    ADX_F64 (float64, the reference GPU path's precision), ADX_F32, ADX_BF16
- *    (tcgen05 tensor-core form with BF16 operands and FP32 accumulation, K <= 16). P/Q
+ *    ADX_F64 (float64, the reference GPU path's precision), ADX_F32, and the tcgen05
+ *    tensor-core form with FP32 accumulation (K <= 16) and BF16 (ADX_BF16) or FP16
+ *    (ADX_F16: power-of-two-scaled operands, 8x finer rounding than BF16) operands. P/Q
  *    passed to a pass are double for ADX_F64 and float otherwise.
  *  - Calls that need scratch memory take a caller-allocated `workspace` whose size
  *    adx_*_workspace_bytes() reports; none of them allocates device memory.
@@ -36,7 +37,7 @@ enum {
   ADX_ERR_TIMEOUT = 5,      /* a bounded in-kernel wait gave up (reported by adx_em_status) */
 };
 
-enum { ADX_F64 = 0, ADX_F32 = 1, ADX_BF16 = 2 };
+enum { ADX_F64 = 0, ADX_F32 = 1, ADX_BF16 = 2, ADX_F16 = 3 };
 
 /* Largest K the kernels accept (the reference's GPU limit, adamixture/entry.py:299-303). */
 #define ADX_MAX_K 64
@@ -129,7 +130,7 @@ int adx_adam_step(double* P, double* Q, const double* P_EM, const double* Q_EM, 
 /* One whole Adam-EM iteration (run_em_step + step) in two launches: the fused E-step
  * sweep, then one kernel that reduces the statistics, forms the EM targets and applies
  * the Adam move to every P and Q row. Inputs of the sweep are P32/Q32 (float) for
- * ADX_F32/ADX_BF16 and P/Q (double) for ADX_F64; P32/Q32 are refreshed. */
+ * ADX_F32/ADX_BF16/ADX_F16 and P/Q (double) for ADX_F64; P32/Q32 are refreshed. */
 int adx_em_adam_iteration(const uint8_t* G, int64_t M, int64_t N, int K, int precision,
                           double* P, double* Q, float* P32, float* Q32, double* mP, double* vP,
                           double* mQ, double* vQ, const double* q_bat, double t, double lr,

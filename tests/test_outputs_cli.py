@@ -86,3 +86,17 @@ def test_cli_parses_reference_options():
         cli.parse_args(["--data_path", "x", "--save_dir", "o", "--name", "n"])
     with pytest.raises(SystemExit):
         cli.parse_args(["--k", "3", "--device", "cpu", "--data_path", "x", "--save_dir", "o", "--name", "n"])
+
+
+def test_precision_policy():
+    """auto: the FP16 tensor-core sweep for 8 <= K <= 16, float32 SIMT otherwise; the
+    tensor-core forms refuse K > 16."""
+    from adamixture_b200.model.em_adam_gpu import resolve_precision
+
+    assert [resolve_precision(K, "auto") for K in (2, 7, 8, 10, 16, 17, 64)] == \
+        ["f32", "f32", "f16", "f16", "f16", "f32", "f32"]
+    assert resolve_precision(10, "mixed") == "f16" and resolve_precision(10, "bf16") == "bf16"
+    for p in ("bf16", "f16"):
+        with pytest.raises(ValueError):
+            resolve_precision(17, p)
+    assert resolve_precision(3, "f64") == "f64"
