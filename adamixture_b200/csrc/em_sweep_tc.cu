@@ -7,9 +7,10 @@
 //   BF16: 8-bit significand, values as they are.
 //   FP16: 11-bit significand (8x finer rounding at the same MMA rate), with power-of-two
 //         scalings that keep every operand in FP16's normal range: P, 1-P and Q are stored
-//         x16 (values >= 1e-5 become >= 1.6e-4; the smallest normal is 6.1e-5), a and b x1/4
-//         (at most 2/1e-5/4 = 5e4 < 65504). H then holds 256 h and A/B/T accumulate 4x their
-//         value; the ratio step and the partial-sum writes undo both scalings exactly.
+//         x8 (values >= 1e-5 become >= 8e-5; the smallest normal is 6.1e-5). H then holds
+//         64 h, so the ratio step's 1/H and 1/Hc are a/64 and b/64 with no extra operation
+//         (from 1/64 up to 2/(64 * 1e-5) = 3125, inside FP16's normal range), and A/B/T
+//         accumulate 1/8 of their value: the partial-sum writes multiply by 8.
 //
 // Per CTA: R = 7 SNP tiles of 128 SNPs (896 SNPs) and a residue class of 128-sample tiles.
 // For each step (sample tile s, SNP tile r), in two half-steps of 64 samples:
@@ -210,9 +211,8 @@ __device__ __forceinline__ uint32_t prmt(uint32_t a, uint32_t b, uint32_t sel) {
 // Operand format traits. GA/GB: the genotype weights g -> {0, 1, 2, 0} (a) and
 // g -> {2, 1, 0, 0} (b) as 16-bit pairs, looked up with one byte permute per pair (entry g
 // at bytes 2g..2g+1 of {hi:lo}). PQ_SCALE: factor on stored P, 1-P and Q; H_UNITS: h in
-// H's units (the 1e-5 clamp is applied there); R_SCALE: factor on 1/(h(1-h)) so the stored
-// ratios carry the 1/4 (FP16); OUT_SCALE: factor that takes the accumulated A/B/T back to
-// their values.
+// H's units (the 1e-5 clamp is applied there); OUT_SCALE: factor that takes the
+// accumulated A/B/T back to their values.
 template <bool F16>
 struct Fmt;
 template <>
@@ -220,7 +220,7 @@ struct Fmt<false> {
   static constexpr uint32_t CODE = 1;  // BF16
   static constexpr uint32_t GA_LO = 0x3F800000u, GA_HI = 0x00004000u;
   static constexpr uint32_t GB_LO = 0x3F804000u, GB_HI = 0x00000000u;
-  static constexpr float PQ_SCALE = 1.0f, H_UNITS = 1.0f, R_SCALE = 1.0f, OUT_SCALE = 1.0f;
+  static constexpr float PQ_SCALE = 1.0f, H_UNITS = 1.0f, OUT_SCALE = 1.0f;
   static __device__ __forceinline__ uint32_t pack(float lo, float hi) {
     uint32_t r;
     asm("cvt.rn.bf16x2.f32 %0, %1, %2;" : "=r"(r) : "f"(hi), "f"(lo));
@@ -237,7 +237,7 @@ struct Fmt<true> {
   static constexpr uint32_t CODE = 0;  // FP16
   static constexpr uint32_t GA_LO = 0x3C000000u, GA_HI = 0x00004000u;
   static constexpr uint32_t GB_LO = 0x3C004000u, GB_HI = 0x00000000u;
-  static constexpr float PQ_SCALE = 16.0f, H_UNITS = 256.0f, R_SCALE = 64.0f, OUT_SCALE = 0.25f;
+  static constexpr float PQ_SCALE = 8.0f, H_UNITS = 64.0f, OUT_SCALE = 8.0f;
   static __device__ __forceinline__ uint32_t pack(float lo, float hi) {
     uint32_t r;
     asm("cvt.rn.f16x2.f32 %0, %1, %2;" : "=r"(r) : "f"(hi), "f"(lo));
@@ -577,9 +577,8 @@ __global__ void __launch_bounds__(TPB, 1) em_sweep_tc_kernel(Args a) {
             const float rec1 = fmaxf(__uint_as_float(hv[cur][e + 1]), ELO);
             const float omr0 = fmaxf(__uint_as_float(cv[cur][e]), ELO);
             const float omr1 = fmaxf(__uint_as_float(cv[cur][e + 1]), ELO);
-            float r0 = rcp_approx(rec0 * omr0), r1 = rcp_approx(rec1 * omr1);
-            if constexpr (F16) { r0 *= F::R_SCALE; r1 *= F::R_SCALE; }
-            const uint32_t ypair = F::pack(omr0 * r0, omr1 * r1);  // 1/rec (FP16: 1/(4 rec))
+            const float r0 = rcp_approx(rec0 * omr0), r1 = rcp_approx(rec1 * omr1);
+            const uint32_t ypair = F::pack(omr0 * r0, omr1 * r1);  // 1/rec (FP16: 1/(64 rec))
             const uint32_t xpair = F::pack(rec0 * r0, rec1 * r1);  // 1/(1-rec)
             ap[e >> 1] = F::mul(prmt(F::GA_LO, F::GA_HI, sel), ypair);
             bp[e >> 1] = F::mul(prmt(F::GB_LO, F::GB_HI, sel), xpair);
