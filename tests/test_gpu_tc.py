@@ -144,3 +144,26 @@ def test_mixed_precision_reaches_the_float32_fit(ops, name, request):
     print(name, "f32", out["f32"], "mixed", out["mixed"])
     L32, Lm = out["f32"][0], out["mixed"][0]
     assert abs(Lm - L32) <= 1e-6 * abs(L32)
+
+
+@pytest.mark.parametrize("K", [1, 2, 3, 5])
+def test_f16_converged_fit_at_small_k(ops, K):
+    # the default E-step for every K <= 16: its converged log-likelihood against this
+    # library's float64 fit (the reference's arithmetic) from the same start
+    from adamixture_b200.model.em_adam_gpu import loglikelihood_gpu, optimize_parameters_gpu
+    from adamixture_b200.src.simulate import make_cohort
+
+    N, M = 1500, 6000
+    coh = make_cohort(N, M, K, F=0.1, alpha=0.5, miss=0.01, seed=70 + K)
+    G = dev_t(orc.pack(coh.genotypes()))
+    rng = np.random.default_rng(K)
+    P0 = rng.uniform(0.2, 0.8, (M, K))
+    Q0 = rng.dirichlet(np.ones(K), N)
+    out = {}
+    for prec in ("f64", "f16"):
+        P, Q = optimize_parameters_gpu(G, dev_t(P0), dev_t(Q0), 0.005, 0.80, 0.88, 1e-8, 10000, 5, K, M, N,
+                                       0.5, 1e-4, 3, 0.1, G.device, 8192, 512, precision=prec)
+        out[prec] = loglikelihood_gpu(G, P, Q, M, N, 8192, G.device, 512)
+    rel = (out["f16"] - out["f64"]) / abs(out["f64"])
+    print("K", K, "f64", out["f64"], "f16", out["f16"], "rel", rel)
+    assert abs(rel) <= 1e-5
