@@ -14,10 +14,11 @@ E-step arithmetic (``precision``): ``"f64"`` reproduces the reference's float64 
 operands, FP32 accumulation; K <= 16); ``"mixed"`` runs tensor-core sweeps until the
 first plateau and float32 sweeps after it. ``set_precision`` sets the default
 (environment: ``ADX_PRECISION``); the default policy ("auto") is ``"f16"`` for
-K <= 16 and ``"f32"`` otherwise. FP16 rather than BF16: at the same cost per iteration,
-its 11-bit operands let Adam converge in float32's number of iterations, where BF16's
-8-bit operands need about twice as many; and the tensor-core sweep is faster than the
-float32 SIMT sweep at every K (1.6x at K=2, 2.8x at K=8 on N=10k x M=200k).
+8 <= K <= 16 and ``"f32"`` otherwise (float32 ratios below K = 8, as specified). FP16
+rather than BF16: at the same cost per iteration, its 11-bit operands let Adam converge
+in float32's number of iterations, where BF16's 8-bit operands need about twice as many.
+``"f16"`` can be asked for at any K <= 16: the tensor-core sweep is also the faster one
+below K = 8 (1.6x at K=2 on N=10k x M=200k).
 """
 from __future__ import annotations
 
@@ -42,12 +43,12 @@ def set_precision(p: str) -> None:
     _PRECISION = p
 
 
-TC_MIN_K, TC_MAX_K = 1, 16
+TC_MIN_K, TC_MAX_K = 8, 16
 
 
 def resolve_precision(K: int, precision: str | None = None) -> str:
     """The E-step arithmetic for this K. "auto": tensor cores (scaled FP16 operands, FP32
-    accumulation) for K <= 16, float32 otherwise. "mixed" resolves to the first
+    accumulation) for 8 <= K <= 16, float32 otherwise. "mixed" resolves to the first
     phase's arithmetic here (the optimiser switches to float32 at the first plateau)."""
     p = precision or _PRECISION
     if p in ("auto", "mixed"):

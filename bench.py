@@ -573,8 +573,8 @@ def run_converge(args, cfg):
 
     fit("plain_f32", P0, Q0, "f32")
     target = max(e[1] for e in runs["plain_f32"]["trace"])
-    fit("bf16", P0, Q0, "bf16" if K <= 16 else "f32")
-    fit("f16", P0, Q0, "f16" if K <= 16 else "f32")
+    fit("bf16", P0, Q0, "bf16" if 8 <= K <= 16 else "f32")
+    fit("f16", P0, Q0, "f16" if 8 <= K <= 16 else "f32")
     fit("mixed", P0, Q0, "mixed")
     net = ws.WarmStartMLP.load(ws.DEFAULT_WEIGHTS, dev)
     torch.cuda.synchronize()

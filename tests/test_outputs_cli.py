@@ -89,12 +89,13 @@ def test_cli_parses_reference_options():
 
 
 def test_precision_policy():
-    """auto: the FP16 tensor-core sweep for K <= 16, float32 SIMT otherwise; the
-    tensor-core forms refuse K > 16."""
+    """auto: the FP16 tensor-core sweep for 8 <= K <= 16, float32 SIMT otherwise; the
+    tensor-core forms take any K <= 16 on request and refuse K > 16."""
     from adamixture_b200.model.em_adam_gpu import resolve_precision
 
     assert [resolve_precision(K, "auto") for K in (1, 2, 7, 8, 10, 16, 17, 64)] == \
-        ["f16", "f16", "f16", "f16", "f16", "f16", "f32", "f32"]
+        ["f32", "f32", "f32", "f16", "f16", "f16", "f32", "f32"]
+    assert resolve_precision(3, "f16") == "f16"
     assert resolve_precision(10, "mixed") == "f16" and resolve_precision(10, "bf16") == "bf16"
     for p in ("bf16", "f16"):
         with pytest.raises(ValueError):
