@@ -440,6 +440,47 @@ def run_e2e(args, G_dev, P0, Q0, M, N, K, prec, dev):
                     "best P/Q copied to the host"}
 
 
+def run_sweep_by_k(args):
+    """Sweep time of the float32 SIMT form against the FP16 tensor-core form for K = 2..16
+    at two shapes (CUDA events, mean of 10 launches after 3 warm-up launches): the
+    measurement behind auto's choice of E-step arithmetic."""
+    import torch
+
+    from adamixture_b200 import ops
+    from adamixture_b200.src.simulate import make_cohort
+
+    dev = torch.device("cuda", 0)
+    out = []
+    for N, M in ((10_000, 200_000), (200_000, 50_000)):
+        for K in (2, 4, 6, 8, 10, 16):
+            coh = make_cohort(N, M, K, 0.05, 0.3, 0.005, 11)
+            Pq = torch.from_numpy(coh.Pq.astype(np.int32)).to(dev)
+            Qq = torch.from_numpy(coh.Qq.astype(np.int32)).to(dev)
+            G = ops.simulate_packed(Pq, Qq, coh.miss_q, coh.keys)
+            del Pq, Qq
+            P = torch.from_numpy(coh.P).to(dev).float().clamp(1e-5, 1 - 1e-5).contiguous()
+            Q = torch.from_numpy(coh.Q).to(dev).float().contiguous()
+            row = {"N": N, "M": M, "K": K}
+            for prec in ("f32", "f16"):
+                ws = torch.zeros(ops.em_workspace_bytes(M, N, K, prec), dtype=torch.uint8, device=dev)
+                for _ in range(3):
+                    ops.em_sweep(G, P, Q, M, prec, ws)
+                s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                torch.cuda.synchronize()
+                s0.record()
+                for _ in range(10):
+                    ops.em_sweep(G, P, Q, M, prec, ws)
+                s1.record()
+                torch.cuda.synchronize()
+                if ops.em_status(ws, M, N, K, prec) != 0:
+                    raise RuntimeError(f"sweep status nonzero at N={N} M={M} K={K} {prec}")
+                row[f"{prec}_ms"] = s0.elapsed_time(s1) / 10
+                del ws
+            out.append(row)
+            del G
+    print(json.dumps({"metric": "E-step sweep ms by K", "rows": out}), flush=True)
+
+
 def run_kernels(args, cfg):
     """Per-kernel timings at the config's shape (CUDA events, mean of ``reps`` launches after
     one warm-up): the randomized-SVD products, the log-likelihood, BVLS, the BR-QN
@@ -650,6 +691,8 @@ def main():
     ap.add_argument("--converge-max-iter", dest="converge_max_iter", type=int, default=300)
     ap.add_argument("--kernels", action="store_true", help="per-kernel timings at the config's shape")
     ap.add_argument("--kernels-skip-hessian", dest="kernels_skip_hessian", action="store_true")
+    ap.add_argument("--sweep-by-k", dest="sweep_by_k", action="store_true",
+                    help="float32 vs FP16 tensor-core sweep time for K = 2..16")
     args = ap.parse_args()
     if args.warmup < 3:
         print("bench.py: --warmup must be >= 3", file=sys.stderr)
@@ -668,6 +711,10 @@ def main():
     if args.kernels:
         if rank == 0:
             run_kernels(args, cfg)
+        return
+    if args.sweep_by_k:
+        if rank == 0:
+            run_sweep_by_k(args)
         return
     run_gpu_arm(args, cfg, rank, world, local_rank)
 
