@@ -40,14 +40,36 @@ __device__ __forceinline__ double renorm(double x, int& e) {
   return __hiloint2double(hi, lo);
 }
 
+// Packed float32 pair: d = a * b + c per lane (fma.rn per lane, as the scalar FMA).
+__device__ __forceinline__ unsigned long long fma_f32x2(unsigned long long a, unsigned long long b,
+                                                        unsigned long long c) {
+  unsigned long long d;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+  return d;
+}
+__device__ __forceinline__ unsigned long long pack_f32x2(float lo, float hi) {
+  unsigned long long r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+  return r;
+}
+__device__ __forceinline__ void unpack_f32x2(unsigned long long v, float& lo, float& hi) {
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+}
+
+// vec: the host checked that N is a multiple of SPT and G is SPT-byte aligned, so a
+// thread's SPT bytes of a packed row are one aligned load.
 template <typename R, int KMAX>
-__global__ void __launch_bounds__(LL_TPB)
+__global__ void __launch_bounds__(LL_TPB, KMAX <= 12 ? 3 : 1)
 loglik_kernel(const uint8_t* __restrict__ G, const R* __restrict__ P, const R* __restrict__ Q,
               int64_t M, int64_t N, int K, int64_t n_stile, int n_split, int n_mblk, int64_t mb,
-              double* __restrict__ partial) {
+              int vec, double* __restrict__ partial) {
   using C = LlCfg<R, KMAX>;
   constexpr int SPT = C::SPT, CH = C::CH;
-  __shared__ R Ps[CH][KMAX];
+  // float32 h of two samples at once with packed FMAs: P is kept duplicated {p, p}
+  constexpr bool PAIRS = sizeof(R) == 4 && SPT % 2 == 0;
+  __shared__ __align__(16) unsigned char ps_raw[CH * KMAX * (PAIRS ? 8 : sizeof(R))];
+  R(*Ps)[KMAX] = reinterpret_cast<R(*)[KMAX]>(ps_raw);
+  unsigned long long(*Ps2)[KMAX] = reinterpret_cast<unsigned long long(*)[KMAX]>(ps_raw);
   __shared__ double wsum[LL_TPB / 32];
   const int mblk = blockIdx.x % n_mblk;
   const int split = blockIdx.x / n_mblk;
@@ -57,49 +79,93 @@ loglik_kernel(const uint8_t* __restrict__ G, const R* __restrict__ P, const R* _
   double acc = 0.0;
   for (int64_t st = split; st < n_stile; st += n_split) {
     const int64_t i0 = st * W + (int64_t)threadIdx.x * SPT;
-    R q[SPT][KMAX];
+    const bool vload = vec && i0 < N;
+    // the thread's SPT bytes of packed row `row` (byte u = sample i0 + u; 0xFF, all
+    // missing, past N)
+    auto load_word = [&](int64_t row) -> uint32_t {
+      const uint8_t* src = G + row * N + i0;
+      if (vload) {
+        if constexpr (SPT == 4) return __ldg(reinterpret_cast<const unsigned int*>(src));
+        else if constexpr (SPT == 2) return (uint32_t)__ldg(reinterpret_cast<const unsigned short*>(src));
+        else return (uint32_t)__ldg(src);
+      }
+      uint32_t w = 0;
+#pragma unroll
+      for (int u = 0; u < SPT; ++u) w |= (i0 + u < N ? (uint32_t)__ldg(src + u) : 0xFFu) << (8 * u);
+      return w;
+    };
+    R q[PAIRS ? 1 : SPT][KMAX];                               // scalar path
+    unsigned long long qp[PAIRS ? SPT / 2 : 1][KMAX];         // packed path: {q_u, q_u+1}
     double prod[SPT];
     int ex[SPT];
+    auto qval = [&](int u, int k) -> R { return (i0 + u < N && k < K) ? Q[(i0 + u) * K + k] : (R)0; };
 #pragma unroll
     for (int u = 0; u < SPT; ++u) {
       prod[u] = 1.0;
       ex[u] = 0;
+    }
+    if constexpr (PAIRS) {
 #pragma unroll
-      for (int k = 0; k < KMAX; ++k) q[u][k] = (i0 + u < N && k < K) ? Q[(i0 + u) * K + k] : (R)0;
+      for (int v = 0; v < SPT / 2; ++v)
+#pragma unroll
+        for (int k = 0; k < KMAX; ++k) qp[v][k] = pack_f32x2((float)qval(2 * v, k), (float)qval(2 * v + 1, k));
+    } else {
+#pragma unroll
+      for (int u = 0; u < SPT; ++u)
+#pragma unroll
+        for (int k = 0; k < KMAX; ++k) q[u][k] = qval(u, k);
     }
     for (int64_t c0 = j0; c0 < j1; c0 += CH) {
       const int cn = (int)min((int64_t)CH, j1 - c0);
       __syncthreads();
       for (int e = threadIdx.x; e < CH * KMAX; e += LL_TPB) {
         const int jl = e / KMAX, k = e % KMAX;
-        Ps[jl][k] = (jl < cn && k < K) ? P[(c0 + jl) * K + k] : (R)0;
+        const R v = (jl < cn && k < K) ? P[(c0 + jl) * K + k] : (R)0;
+        if constexpr (PAIRS) Ps2[jl][k] = pack_f32x2((float)v, (float)v);
+        else Ps[jl][k] = v;
       }
       __syncthreads();
+      uint32_t word = load_word(c0 >> 2);
       for (int qd = 0; qd < cn; qd += 4) {
-        const int64_t row = (c0 + qd) >> 2;
-        uint32_t bytes[SPT];
-#pragma unroll
-        for (int u = 0; u < SPT; ++u) bytes[u] = (i0 + u < N) ? (uint32_t)__ldg(G + row * N + i0 + u) : 0xFFu;
+        const uint32_t cur = word;
+        if (qd + 4 < cn) word = load_word((c0 + qd + 4) >> 2);  // next quad, ahead of the math
 #pragma unroll
         for (int s = 0; s < 4; ++s) {
           const int jl = qd + s;
           if (jl >= cn) break;
+          R h[SPT];
+          if constexpr (PAIRS) {
+#pragma unroll
+            for (int v = 0; v < SPT / 2; ++v) {
+              unsigned long long a2 = 0ull;
+#pragma unroll
+              for (int k = 0; k < KMAX; ++k) a2 = fma_f32x2(Ps2[jl][k], qp[v][k], a2);
+              float lo, hi;
+              unpack_f32x2(a2, lo, hi);
+              h[2 * v] = lo;
+              h[2 * v + 1] = hi;
+            }
+          } else {
+#pragma unroll
+            for (int u = 0; u < SPT; ++u) {
+              h[u] = 0;
+#pragma unroll
+              for (int k = 0; k < KMAX; ++k) h[u] += Ps[jl][k] * q[u][k];
+            }
+          }
 #pragma unroll
           for (int u = 0; u < SPT; ++u) {
-            const unsigned g = genotype(bytes[u], s);
-            R h = 0;
-#pragma unroll
-            for (int k = 0; k < KMAX; ++k) h += Ps[jl][k] * q[u][k];
+            const unsigned g = genotype(cur >> (8 * u), s);
             if constexpr (sizeof(R) == 4) {
               // float32 h: the factor in float32 as well (its rounding, 6e-8 relative, is below
               // that of h itself); the clamp h in [1e-10, 1-1e-10] is applied to h and to 1-h,
               // since 1-1e-10 is not a float32 value; f >= 1e-20 stays a normal float
-              const float hf = fmaxf(h, (float)LL_CLAMP);
-              const float om = fmaxf(1.0f - h, (float)LL_CLAMP);
+              const float hf = fmaxf(h[u], (float)LL_CLAMP);
+              const float om = fmaxf(1.0f - h[u], (float)LL_CLAMP);
               const float f = g == 0u ? om * om : (g == 1u ? hf * om : (g == 2u ? hf * hf : 1.0f));
               prod[u] *= (double)f;
             } else {
-              const double hd = fmin(fmax((double)h, LL_CLAMP), 1.0 - LL_CLAMP);
+              const double hd = fmin(fmax((double)h[u], LL_CLAMP), 1.0 - LL_CLAMP);
               const double om = 1.0 - hd;
               const double f = g == 0u ? om * om : (g == 1u ? hd * om : (g == 2u ? hd * hd : 1.0));
               prod[u] *= f;
@@ -159,6 +225,12 @@ static int spt_of() { return LlCfg<R, KMAX>::SPT; }
     default: break;                                                                    \
   }
 
+// Whether a thread's SPT bytes of a packed row can be one aligned load: N a multiple of
+// SPT (so every row starts SPT-aligned relative to G) and G itself SPT-byte aligned.
+static int ll_vec_loads(const uint8_t* G, int64_t N, int spt) {
+  return (N % spt == 0) && (reinterpret_cast<uintptr_t>(G) % (uintptr_t)spt == 0) ? 1 : 0;
+}
+
 static int ll_plan(int64_t M, int64_t N, int K, int prec, LlPlan& pl) {
   if (M <= 0 || N <= 0 || K < 1 || K > ADX_MAX_K) return ADX_ERR_ARG;
   if (prec != ADX_F64 && prec != ADX_F32 && prec != ADX_BF16 && prec != ADX_F16) return ADX_ERR_UNSUPPORTED;
@@ -206,8 +278,9 @@ extern "C" int adx_loglik(const uint8_t* G, int64_t M, int64_t N, int K, int pre
   if (workspace_bytes < (size_t)nblk * sizeof(double)) { adx_set_message("adx_loglik: workspace too small"); return ADX_ERR_WORKSPACE; }
   double* part = reinterpret_cast<double*>(workspace);
   cudaStream_t st = as_stream(stream);
-#define L64(KM) loglik_kernel<double, KM><<<nblk, LL_TPB, 0, st>>>(G, (const double*)P, (const double*)Q, M, N, K, pl.n_stile, pl.n_split, pl.n_mblk, pl.mb, part)
-#define L32(KM) loglik_kernel<float, KM><<<nblk, LL_TPB, 0, st>>>(G, (const float*)P, (const float*)Q, M, N, K, pl.n_stile, pl.n_split, pl.n_mblk, pl.mb, part)
+  const int vec = ll_vec_loads(G, N, pl.spt);
+#define L64(KM) loglik_kernel<double, KM><<<nblk, LL_TPB, 0, st>>>(G, (const double*)P, (const double*)Q, M, N, K, pl.n_stile, pl.n_split, pl.n_mblk, pl.mb, vec, part)
+#define L32(KM) loglik_kernel<float, KM><<<nblk, LL_TPB, 0, st>>>(G, (const float*)P, (const float*)Q, M, N, K, pl.n_stile, pl.n_split, pl.n_mblk, pl.mb, vec, part)
   if (precision == ADX_F64) { ADX_LL_KMAX_SWITCH(pl.kmax, L64) } else { ADX_LL_KMAX_SWITCH(pl.kmax, L32) }
 #undef L64
 #undef L32
@@ -282,8 +355,9 @@ extern "C" int adx_loglik_noalloc(const uint8_t* G, int64_t M, int64_t N, int K,
   rc = ll_noalloc_scratch(&part);
   if (rc) return rc;
   cudaStream_t st = as_stream(stream);
-#define N64(KM) loglik_kernel<double, KM><<<nblk, LL_TPB, 0, st>>>(G, (const double*)P, (const double*)Q, M, N, K, pl.n_stile, pl.n_split, pl.n_mblk, pl.mb, part)
-#define N32(KM) loglik_kernel<float, KM><<<nblk, LL_TPB, 0, st>>>(G, (const float*)P, (const float*)Q, M, N, K, pl.n_stile, pl.n_split, pl.n_mblk, pl.mb, part)
+  const int vec = ll_vec_loads(G, N, pl.spt);
+#define N64(KM) loglik_kernel<double, KM><<<nblk, LL_TPB, 0, st>>>(G, (const double*)P, (const double*)Q, M, N, K, pl.n_stile, pl.n_split, pl.n_mblk, pl.mb, vec, part)
+#define N32(KM) loglik_kernel<float, KM><<<nblk, LL_TPB, 0, st>>>(G, (const float*)P, (const float*)Q, M, N, K, pl.n_stile, pl.n_split, pl.n_mblk, pl.mb, vec, part)
   if (precision == ADX_F64) { ADX_LL_KMAX_SWITCH(pl.kmax, N64) } else { ADX_LL_KMAX_SWITCH(pl.kmax, N32) }
 #undef N64
 #undef N32

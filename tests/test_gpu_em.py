@@ -245,6 +245,30 @@ def test_loglik(ops, name, request):
     assert abs(l32 - ref) <= 1e-6 * abs(ref)
 
 
+@pytest.mark.parametrize("N,M,K", [(1024, 777, 10), (1026, 501, 8), (4000, 333, 3), (2048, 130, 16),
+                                   (512, 64, 24), (1000, 97, 64)])
+def test_loglik_load_paths(ops, N, M, K):
+    # N a multiple of the samples per thread: one word load per packed quad; otherwise, or
+    # with G one byte off alignment, byte loads. Same sums either way, and against the oracle.
+    rng = np.random.default_rng(N + M + K)
+    G = rng.choice(4, size=(M, N), p=[0.3, 0.35, 0.3, 0.05]).astype(np.uint8)
+    P = np.clip(rng.beta(0.8, 0.8, size=(M, K)), 1e-5, 1 - 1e-5)
+    Q = rng.dirichlet(np.full(K, 0.5), size=N)
+    ref = orc.loglik(G, P, Q)
+    Gp = orc.pack(G)
+    Gd = dev_t(Gp)
+    flat = torch.empty(Gp.size + 1, dtype=torch.uint8, device=Gd.device)
+    flat[1:] = Gd.reshape(-1)
+    Gmis = flat[1:].view(Gp.shape)
+    for prec, tol in (("f64", 1e-12), ("f32", 1e-6)):
+        dt = torch.float64 if prec == "f64" else torch.float32
+        Pd, Qd = dev_t(P, dt), dev_t(Q, dt)
+        a = float(ops.loglik_device(Gd, Pd, Qd, M, prec).item())
+        b = float(ops.loglik_device(Gmis, Pd, Qd, M, prec).item())
+        assert a == b, (prec, a, b)
+        assert abs(a - ref) <= tol * abs(ref), (prec, a, ref)
+
+
 @pytest.mark.parametrize("prec", ["f64", "f32"])
 @pytest.mark.parametrize("name", ["demo", "synth"])
 def test_converged_loglik_within_1e6(ops, name, prec, request):
