@@ -7,8 +7,12 @@
 // summed over the held-out entries. Folds come either as a list of flat indices j*N + i
 // (the reference's shuffled-list rule, drawn on the host with its generator) or from the
 // reference's deterministic hash of the flat index (cv.py:58-78), evaluated here per entry
-// so no index list is built. Hiding sets the entry's two bits to 3 with an atomic OR on the
-// containing 32-bit word (entries of one byte may be hidden by different threads).
+// so no index list is built. From a list, hiding sets the entry's two bits to 3 with an
+// atomic OR on the containing 32-bit word (entries of one byte may be hidden by different
+// threads). The hash rule runs one thread per packed byte (SNPs 4r..4r+3 of sample i, rows
+// over blocks, samples over threads): the flat index j*N + i is a multiply-add, the thread
+// owns its byte (no atomics), and for 2..16 folds the fold count is a compile-time constant
+// so the hash's modulo is a multiply-high sequence, not a 64-bit division.
 // Deviance sums are float64 per-block partials added in a fixed order.
 #include "common.cuh"
 
@@ -18,14 +22,22 @@ namespace cv {
 constexpr int TPB = 256;
 constexpr int BLOCKS = 1184;   // partials of a deviance sum (8 per SM on 148 SMs)
 
-__device__ __forceinline__ bool hash_in_fold(uint64_t flat, uint64_t seed, uint64_t n_folds, uint64_t fold) {
+__device__ __forceinline__ uint64_t fold_hash(uint64_t flat, uint64_t seed) {
   uint64_t h = flat + seed + 0x9E3779B97F4A7C15ull;
   h ^= h >> 30;
   h *= 0xBF58476D1CE4E5B9ull;
   h ^= h >> 27;
   h *= 0x94D049BB133111EBull;
   h ^= h >> 31;
-  return h % n_folds == fold;
+  return h;
+}
+
+// NF > 0: the fold count as a constant; NF == 0: n_folds at run time.
+template <int NF>
+__device__ __forceinline__ bool in_fold(uint64_t flat, uint64_t seed, uint64_t n_folds, uint64_t fold) {
+  const uint64_t h = fold_hash(flat, seed);
+  if constexpr (NF > 0) return h % (uint64_t)NF == fold;
+  else return h % n_folds == fold;
 }
 
 __device__ __forceinline__ void hide(uint8_t* G, int64_t N, int64_t j, int64_t i) {
@@ -61,12 +73,22 @@ __global__ void mask_list_kernel(uint8_t* G, int64_t M, int64_t N, const int64_t
 }
 
 // Every (j, i) with g != 3 in the unmasked G0 and the fold's hash; hidden in G.
+template <int NF>
 __global__ void mask_hash_kernel(uint8_t* G, const uint8_t* __restrict__ G0, int64_t M, int64_t N, uint64_t seed,
                                  uint64_t n_folds, uint64_t fold) {
-  const int64_t total = M * N;
-  for (int64_t f = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; f < total; f += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t j = f / N, i = f - j * N;
-    if (geno(G0, N, j, i) != 3u && hash_in_fold((uint64_t)f, seed, n_folds, fold)) hide(G, N, j, i);
+  const int64_t rows = (M + 3) >> 2;
+  for (int64_t r = blockIdx.x; r < rows; r += gridDim.x) {
+    const int ns = (int)min((int64_t)4, M - 4 * r);
+    for (int64_t i = threadIdx.x; i < N; i += blockDim.x) {
+      const int64_t b = r * N + i;
+      const unsigned byte = G0[b];
+      const uint64_t f0 = (uint64_t)(4 * r) * (uint64_t)N + (uint64_t)i;
+      unsigned mask = 0u;
+      for (int s = 0; s < ns; ++s)
+        if (((byte >> (2 * s)) & 3u) != 3u && in_fold<NF>(f0 + (uint64_t)s * (uint64_t)N, seed, n_folds, fold))
+          mask |= 3u << (2 * s);
+      if (mask) G[b] = (uint8_t)(G[b] | mask);
+    }
   }
 }
 
@@ -97,15 +119,23 @@ __global__ void __launch_bounds__(TPB) dev_list_kernel(const uint8_t* __restrict
   block_sum_to(acc, part);
 }
 
+template <int NF>
 __global__ void __launch_bounds__(TPB) dev_hash_kernel(const uint8_t* __restrict__ G0, int64_t M, int64_t N, int K,
                                                        const double* __restrict__ P, const double* __restrict__ Q,
                                                        uint64_t seed, uint64_t n_folds, uint64_t fold, double* part) {
   double acc = 0.0;
-  const int64_t total = M * N;
-  for (int64_t f = (int64_t)blockIdx.x * TPB + threadIdx.x; f < total; f += (int64_t)gridDim.x * TPB) {
-    const int64_t j = f / N, i = f - j * N;
-    const unsigned g = geno(G0, N, j, i);
-    if (g != 3u && hash_in_fold((uint64_t)f, seed, n_folds, fold)) acc += deviance(P, Q, K, j, i, g);
+  const int64_t rows = (M + 3) >> 2;
+  for (int64_t r = blockIdx.x; r < rows; r += gridDim.x) {
+    const int ns = (int)min((int64_t)4, M - 4 * r);
+    for (int64_t i = threadIdx.x; i < N; i += TPB) {
+      const unsigned byte = G0[r * N + i];
+      const uint64_t f0 = (uint64_t)(4 * r) * (uint64_t)N + (uint64_t)i;
+      for (int s = 0; s < ns; ++s) {
+        const unsigned g = (byte >> (2 * s)) & 3u;
+        if (g != 3u && in_fold<NF>(f0 + (uint64_t)s * (uint64_t)N, seed, n_folds, fold))
+          acc += deviance(P, Q, K, 4 * r + s, i, g);
+      }
+    }
   }
   block_sum_to(acc, part);
 }
@@ -124,6 +154,17 @@ __global__ void sum_kernel(const double* part, int n, double* out) {
 using namespace adx;
 
 static bool cv_args_ok(const void* G, int64_t M, int64_t N) { return G && M > 0 && N > 0; }
+
+// Fold counts 2..16 as compile-time constants, anything else at run time.
+#define ADX_CV_FOLD_SWITCH(nf, MACRO)                                                      \
+  switch (nf) {                                                                            \
+    case 2: MACRO(2); break;   case 3: MACRO(3); break;   case 4: MACRO(4); break;         \
+    case 5: MACRO(5); break;   case 6: MACRO(6); break;   case 7: MACRO(7); break;         \
+    case 8: MACRO(8); break;   case 9: MACRO(9); break;   case 10: MACRO(10); break;       \
+    case 11: MACRO(11); break; case 12: MACRO(12); break; case 13: MACRO(13); break;       \
+    case 14: MACRO(14); break; case 15: MACRO(15); break; case 16: MACRO(16); break;       \
+    default: MACRO(0); break;                                                              \
+  }
 
 // The masked copy is written by 32-bit atomics: it must start on a 4-byte boundary and its
 // allocation (g_bytes) must cover the packed matrix rounded up to whole words.
@@ -168,8 +209,10 @@ extern "C" int adx_cv_mask_hash(uint8_t* G, size_t g_bytes, const uint8_t* G0, i
     return ADX_ERR_ARG;
   }
   const int64_t blocks = (int64_t)sm_count() * 8;
-  cv::mask_hash_kernel<<<(unsigned)blocks, 256, 0, as_stream(stream)>>>(G, G0, M, N, seed, (uint64_t)n_folds,
-                                                                          (uint64_t)fold);
+  cudaStream_t st = as_stream(stream);
+#define ADX_MASK(NF) cv::mask_hash_kernel<NF><<<(unsigned)blocks, 256, 0, st>>>(G, G0, M, N, seed, (uint64_t)n_folds, (uint64_t)fold)
+  ADX_CV_FOLD_SWITCH(n_folds, ADX_MASK)
+#undef ADX_MASK
   ADX_LAUNCH_CHECK();
   return ADX_OK;
 }
@@ -206,7 +249,9 @@ extern "C" int adx_cv_deviance_hash(const uint8_t* G0, int64_t M, int64_t N, int
   if (!workspace || workspace_bytes < need) { adx_set_message("adx_cv_deviance_hash: workspace too small"); return ADX_ERR_WORKSPACE; }
   cudaStream_t st = as_stream(stream);
   double* part = static_cast<double*>(workspace);
-  cv::dev_hash_kernel<<<cv::BLOCKS, cv::TPB, 0, st>>>(G0, M, N, K, P, Q, seed, (uint64_t)n_folds, (uint64_t)fold, part);
+#define ADX_DEV(NF) cv::dev_hash_kernel<NF><<<cv::BLOCKS, cv::TPB, 0, st>>>(G0, M, N, K, P, Q, seed, (uint64_t)n_folds, (uint64_t)fold, part)
+  ADX_CV_FOLD_SWITCH(n_folds, ADX_DEV)
+#undef ADX_DEV
   ADX_LAUNCH_CHECK();
   cv::sum_kernel<<<1, 32, 0, st>>>(part, cv::BLOCKS, out);
   ADX_LAUNCH_CHECK();

@@ -59,6 +59,32 @@ def test_mask_list_and_hash(ops, cv_proj):
     assert abs(d_hash - osv.deviance_sum(G, cv_proj["P"], cv_proj["Q"], allf[hide])) <= 1e-12 * abs(d_hash)
 
 
+@pytest.mark.parametrize("M,N,n_folds,fold", [(701, 90, 5, 0), (701, 90, 17, 16), (333, 1001, 3, 2),
+                                              (66, 50, 16, 7), (5, 7, 2, 1)])
+def test_hash_folds_ragged_and_runtime_count(ops, M, N, n_folds, fold):
+    # a partial last packed row (M % 4 != 0), fold counts compiled as constants (2..16) and
+    # one taken at run time (17): the hidden entries and the deviance against the reference's
+    # hash rule restated on the host
+    from adamixture_b200.src import cv
+
+    rng = np.random.default_rng(M * N + n_folds)
+    G = rng.choice(4, size=(M, N), p=[0.3, 0.35, 0.3, 0.05]).astype(np.uint8)
+    K = 4
+    P = np.clip(rng.beta(0.8, 0.8, size=(M, K)), 1e-5, 1 - 1e-5)
+    Q = rng.dirichlet(np.full(K, 0.5), size=N)
+    Gd = dev(orc.pack(G))
+    Gh = ops.masked_copy(Gd)
+    ops.cv_mask_hash(Gh, Gd, M, 7, n_folds, fold)
+    allf = np.arange(M * N)
+    hide = cv.hash_fold_mask(allf, 7, n_folds, fold) & (G.reshape(-1) != 3)
+    want = G.copy().reshape(-1)
+    want[hide] = 3
+    np.testing.assert_array_equal(Gh.cpu().numpy(), orc.pack(want.reshape(M, N)))
+    d_hash = ops.cv_deviance_hash(Gd, dev(P), dev(Q), M, 7, n_folds, fold)
+    ref = osv.deviance_sum(G, P, Q, allf[hide])
+    assert abs(d_hash - ref) <= 1e-12 * max(abs(ref), 1.0)
+
+
 def test_cv_index_matches_reference(cuda, cv_proj):
     from adamixture_b200.src.cv import run_cross_validation
 
