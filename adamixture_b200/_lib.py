@@ -41,8 +41,6 @@ SIGNATURES: dict[str, list] = {
                       c_double, c_double, P, P, P],
     "adx_em_adam_iteration": [P, I64, I64, c_int, c_int, P, P, P, P, P, P, P, P, P, c_double,
                               c_double, c_double, c_double, c_double, P, c_size_t, P],
-    "adx_em_adam_update": [I64, I64, c_int, c_int, P, P, P, P, P, P, P, P, P, c_double, c_double,
-                           c_double, c_double, c_double, P, c_size_t, P],
     "adx_loglik_workspace_bytes": [I64, I64, c_int, c_int, P],
     "adx_loglik": [P, I64, I64, c_int, c_int, P, P, P, P, c_size_t, P],
     "adx_loglik_noalloc": [P, I64, I64, c_int, c_int, P, P, P, P],

@@ -615,25 +615,3 @@ extern "C" int adx_em_adam_iteration(const uint8_t* G, int64_t M, int64_t N, int
   return em_update(pl, workspace, 1, nullptr, nullptr, nullptr, q_bat, P, Q, P32, Q32, mP, vP, mQ,
                    vQ, AdamArgs{t, lr, beta1, beta2, eps}, st);
 }
-
-// The second launch of adx_em_adam_iteration alone: the statistics from the partials that
-// the last adx_em_sweep left in this workspace (same shape and precision), the EM targets
-// and the Adam move. Splitting the iteration lets a caller launch other work that reads
-// the same P/Q (a log-likelihood check) between the sweep and the move.
-extern "C" int adx_em_adam_update(int64_t M, int64_t N, int K, int precision, double* P, double* Q,
-                                  float* P32, float* Q32, double* mP, double* vP, double* mQ,
-                                  double* vQ, const double* q_bat, double t, double lr, double beta1,
-                                  double beta2, double eps, void* workspace, size_t workspace_bytes,
-                                  void* stream) {
-  EmPlan pl;
-  int rc = em_plan(M, N, K, precision, pl);
-  if (rc) { adx_set_message("adx_em_adam_update: bad shape or precision"); return rc; }
-  if (!P || !Q || !mP || !vP || !mQ || !vQ || !q_bat || !workspace || t < 1) {
-    adx_set_message("adx_em_adam_update: bad arguments");
-    return ADX_ERR_ARG;
-  }
-  if (precision != ADX_F64 && (!P32 || !Q32)) { adx_set_message("adx_em_adam_update: P32/Q32 required"); return ADX_ERR_ARG; }
-  if (workspace_bytes < pl.bytes()) { adx_set_message("adx_em_adam_update: workspace too small"); return ADX_ERR_WORKSPACE; }
-  return em_update(pl, workspace, 1, nullptr, nullptr, nullptr, q_bat, P, Q, P32, Q32, mP, vP, mQ,
-                   vQ, AdamArgs{t, lr, beta1, beta2, eps}, as_stream(stream));
-}

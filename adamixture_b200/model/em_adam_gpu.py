@@ -137,19 +137,6 @@ class EMAdamOptimizer:
         ops.adam_step(P, Q, P_target, Q_target, self.m_P, self.v_P, self.m_Q, self.v_Q,
                       self._t, self.lr, self.beta1, self.beta2, self.reg_adam, P32, Q32)
 
-    def sweep(self, G, P, Q, P32, Q32, M, workspace):
-        """The E-step sweep of the next ``fused_iteration`` alone (partials in ``workspace``)."""
-        self._sample_counts(G, M)
-        Pin, Qin = (P, Q) if self.precision == "f64" else (P32, Q32)
-        ops.em_sweep(G, Pin, Qin, M, self.precision, workspace)
-
-    def update(self, P, Q, P32, Q32, M, workspace):
-        """The rest of the iteration whose sweep ``sweep`` launched: targets and Adam move."""
-        self._t += 1
-        ops.em_adam_update(P, Q, P32, Q32, self.m_P, self.v_P, self.m_Q, self.v_Q, self.q_bat, M,
-                           self._t, self.lr, self.beta1, self.beta2, self.reg_adam, self.precision,
-                           workspace)
-
     def fused_iteration(self, G, P, Q, P32, Q32, M, workspace=None):
         """``run_em_step`` + ``step`` in two launches, without materialising A/B/T."""
         self._sample_counts(G, M)
@@ -180,7 +167,7 @@ def loglikelihood_gpu(G, P, Q, M, N, batch_size, device, threads_per_block, prec
 
 def _optimize_parameters_gpu_once(G, P, Q, lr, beta1, beta2, reg_adam, max_iter, check, K, M, N,
                                   lr_decay, min_lr, patience, tol_adam, device, chunk_size,
-                                  threads_per_block, precision=None, trace=None, overlap_check=True):
+                                  threads_per_block, precision=None, trace=None):
     """Adam-EM with lr decay (em_adam_gpu.py:281-356), fused iterations.
 
     Same control flow as the reference: priming (E-step + Adam step), log-likelihood of
@@ -188,16 +175,9 @@ def _optimize_parameters_gpu_once(G, P, Q, lr, beta1, beta2, reg_adam, max_iter,
     ``check`` iterations. The reference's second priming E-step, whose result it never
     uses (:322), is skipped: it changes no state. ``trace`` (a list) receives
     ``(iteration, loglik, seconds since the start)`` at each check (host clock after the
-    check's read-back, so the device work up to it is included). ``precision="mixed"``:
-    tensor-core sweeps until the first plateau (``patience`` checks without a new best),
-    float32 sweeps after it, with the same Adam state and learning rate.
-
-    ``overlap_check``: the log-likelihood check of an iterate and the next iteration's
-    E-step sweep only read P/Q, so the check runs on a second stream concurrently with that
-    sweep (the loop's own stream has the higher priority, so the sweep's blocks are placed
-    first); the host reads the log-likelihood before it launches the Adam move that depends
-    on it. Same arithmetic and decisions as without the overlap; when the loop stops at a
-    check, the sweep launched beside that check is discarded.
+    check's read-back, so the device work up to it is included). ``precision="mixed"``: tensor-core (BF16) sweeps
+    until the first plateau (``patience`` checks without a new best), float32 sweeps after
+    it, with the same Adam state and learning rate.
     """
     mixed = (precision or _PRECISION) == "mixed"
     opt = EMAdamOptimizer(P.shape, Q.shape, lr, beta1, beta2, reg_adam, device, precision)
@@ -207,100 +187,71 @@ def _optimize_parameters_gpu_once(G, P, Q, lr, beta1, beta2, reg_adam, max_iter,
     P32 = P.to(torch.float32).contiguous() if dt == torch.float32 else None
     Q32 = Q.to(torch.float32).contiguous() if dt == torch.float32 else None
     ws = ops.Workspace.get(G.device, ops.em_workspace_bytes(M, N, K, prec))
-    caller = torch.cuda.current_stream(G.device)
-    main = torch.cuda.Stream(device=G.device, priority=-1) if overlap_check else caller
-    side = torch.cuda.Stream(device=G.device) if overlap_check else None
 
-    def launch_loglik():
-        Pl, Ql = (P, Q) if ll_prec == "f64" else (P32, Q32)
-        if side is None:
-            return ops.loglik_device(G, Pl, Ql, M, ll_prec)
-        side.wait_stream(main)
-        with torch.cuda.stream(side):
-            return ops.loglik_device(G, Pl, Ql, M, ll_prec)
-
-    def read(out):
-        if side is None:
-            L = float(out.item())
+    def loglik():
+        if ll_prec == "f64":
+            L = float(ops.loglik_device(G, P, Q, M, "f64").item())
         else:
-            with torch.cuda.stream(side):
-                L = float(out.item())
+            L = float(ops.loglik_device(G, P32, Q32, M, "f32").item())
         st = ops.em_status(ws, M, N, K, prec)
         if st:
             raise RuntimeError(f"E-step sweep reported status {st} (a bounded wait timed out)")
         return L
 
-    main.wait_stream(caller)
-    with torch.cuda.stream(main):
-        ts = time.time()
-        t_start = time.perf_counter()
+    ts = time.time()
+    t_start = time.perf_counter()
+    opt.fused_iteration(G, P, Q, P32, Q32, M, ws)
+    log.info(f"    Performed priming iteration... ({time.time() - ts:.1f}s)\n")
+    L_best = loglik()
+    P_best, Q_best = P.clone(), Q.clone()
+    wait_lr = 0
+    ts = time.time()
+    for it in range(max_iter):
         opt.fused_iteration(G, P, Q, P32, Q32, M, ws)
-        log.info(f"    Performed priming iteration... ({time.time() - ts:.1f}s)\n")
-        L_best = read(launch_loglik())
-        P_best, Q_best = P.clone(), Q.clone()
-        wait_lr = 0
-        swept = False   # this iteration's sweep already launched beside the last check
-        ts = time.time()
-        for it in range(max_iter):
-            if not swept:
-                opt.sweep(G, P, Q, P32, Q32, M, ws)
-            swept = False
-            opt.update(P, Q, P32, Q32, M, ws)
-            if (it + 1) % check == 0:
-                out = launch_loglik()
-                if side is not None and it + 1 < max_iter:
-                    opt.sweep(G, P, Q, P32, Q32, M, ws)
-                    swept = True
-                L_cur = read(out)
-                if trace is not None:
-                    trace.append((it + 1, L_cur, time.perf_counter() - t_start))
-                log.info(f"    Iteration {it+1}, Log-likelihood: {L_cur:.1f}, Time: {time.time() - ts:.3f}s")
-                ts = time.time()
-                if L_cur > L_best + tol_adam:
-                    L_best = L_cur
-                    P_best.copy_(P)
-                    Q_best.copy_(Q)
+        if (it + 1) % check == 0:
+            L_cur = loglik()
+            if trace is not None:
+                trace.append((it + 1, L_cur, time.perf_counter() - t_start))
+            log.info(f"    Iteration {it+1}, Log-likelihood: {L_cur:.1f}, Time: {time.time() - ts:.3f}s")
+            ts = time.time()
+            if L_cur > L_best + tol_adam:
+                L_best = L_cur
+                P_best.copy_(P)
+                Q_best.copy_(Q)
+                wait_lr = 0
+            else:
+                wait_lr += 1
+                if wait_lr >= patience and mixed and prec != "f32":
+                    # mixed precision: the first plateau ends the BF16 phase; the same Adam
+                    # state continues with float32 sweeps (same float32 P/Q shadows)
+                    prec = opt.precision = "f32"
+                    ws = ops.Workspace.get(G.device, ops.em_workspace_bytes(M, N, K, prec))
+                    log.info("    Plateau in the BF16 phase: continuing with float32 E-steps.")
                     wait_lr = 0
-                else:
-                    wait_lr += 1
-                    if wait_lr >= patience and mixed and prec != "f32":
-                        # mixed precision: the first plateau ends the tensor-core phase; the same
-                        # Adam state continues with float32 sweeps (same float32 P/Q shadows)
-                        prec = opt.precision = "f32"
-                        ws = ops.Workspace.get(G.device, ops.em_workspace_bytes(M, N, K, prec))
-                        swept = False   # the sweep beside this check used the old arithmetic
-                        log.info("    Plateau in the tensor-core phase: continuing with float32 E-steps.")
-                        wait_lr = 0
-                        continue
-                    if wait_lr >= patience:
-                        old = opt.lr
-                        opt.lr = max(opt.lr * lr_decay, min_lr)
-                        log.info(f"    Plateau reached ({wait_lr} checks without beating best). "
-                                 f"Reducing lr: {old:.3e} → {opt.lr:.3e}")
-                        if opt.lr <= min_lr:
-                            log.info("        Convergence reached.")
-                            break
-                        wait_lr = 0
-    caller.wait_stream(main)
-    if side is not None:
-        P_best.record_stream(caller)
-        Q_best.record_stream(caller)
+                    continue
+                if wait_lr >= patience:
+                    old = opt.lr
+                    opt.lr = max(opt.lr * lr_decay, min_lr)
+                    log.info(f"    Plateau reached ({wait_lr} checks without beating best). "
+                             f"Reducing lr: {old:.3e} → {opt.lr:.3e}")
+                    if opt.lr <= min_lr:
+                        log.info("        Convergence reached.")
+                        break
+                    wait_lr = 0
     log.info(f"\n    Final log-likelihood: {L_best:.1f}")
     return P_best, Q_best
 
 
 def optimize_parameters_gpu(G, P, Q, lr, beta1, beta2, reg_adam, max_iter, check, K, M, N,
                             lr_decay, min_lr, patience, tol_adam, device, chunk_size,
-                            threads_per_block, precision=None, trace=None, overlap_check=True):
+                            threads_per_block, precision=None, trace=None):
     """Adam-EM on the GPU (em_adam_gpu.py:359-385). The reference's OOM retry halves the
     chunk size; the fused sweep has no per-chunk temporaries, so there is nothing to
-    retry: the only allocations are P/Q-sized buffers and the partial-sum workspace.
-    ``overlap_check``: run each log-likelihood check beside the next sweep (same results)."""
+    retry: the only allocations are P/Q-sized buffers and the partial-sum workspace."""
     _require_cuda(G, P, Q)
     P = P.to(torch.float64).contiguous().clone()
     Q = Q.to(torch.float64).contiguous().clone()
     return _optimize_parameters_gpu_once(G, P, Q, lr, beta1, beta2, reg_adam, max_iter, check, K,
                                          M, N, lr_decay, min_lr, patience, tol_adam, device,
-                                         chunk_size, threads_per_block, precision, trace,
-                                         overlap_check)
+                                         chunk_size, threads_per_block, precision, trace)
 

@@ -217,18 +217,6 @@ def adam_step(P, Q, P_EM, Q_EM, mP, vP, mQ, vQ, t, lr, beta1, beta2, eps, P32=No
          float(lr), float(beta1), float(beta2), float(eps), _ptr(P32), _ptr(Q32), _stream(P.device))
 
 
-def em_adam_update(P, Q, P32, Q32, mP, vP, mQ, vQ, q_bat, M, t, lr, beta1, beta2, eps, precision,
-                   workspace: torch.Tensor):
-    """The update half of ``em_adam_iteration`` (statistics from the partials the last
-    ``em_sweep`` left in ``workspace``, EM targets, Adam move), in place."""
-    pc = precision_code(precision)
-    N, K = Q.shape
-    call("adx_em_adam_update", M, N, K, pc, P.data_ptr(), Q.data_ptr(), _ptr(P32), _ptr(Q32),
-         mP.data_ptr(), vP.data_ptr(), mQ.data_ptr(), vQ.data_ptr(), q_bat.data_ptr(), float(t),
-         float(lr), float(beta1), float(beta2), float(eps), workspace.data_ptr(), workspace.numel(),
-         _stream(P.device))
-
-
 def em_adam_iteration(G, P, Q, P32, Q32, mP, vP, mQ, vQ, q_bat, M, t, lr, beta1, beta2, eps,
                       precision="f32", workspace: torch.Tensor | None = None):
     """One fused Adam-EM iteration (E-step sweep + targets + Adam move), in place."""

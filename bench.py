@@ -264,42 +264,25 @@ def run_gpu_arm(args, cfg, rank, world, local_rank):
     Pll, Qll = (P, Q) if llp == "f64" else (P32, Q32)
     launches = {"n": 0}
 
-    step_stream = torch.cuda.current_stream(dev)
     if not sharded:
-        # the optimiser's loop (optimize_parameters_gpu): per iteration the sweep (+ the 16-bit
-        # copy of Q for the tensor-core sweep) and the update kernel; per check the
-        # log-likelihood kernel and its final sum on a second stream, beside the next
-        # iteration's sweep (launched ahead, except after the last timed step)
+        # kernels per fused iteration: sweep (+ the BF16 copy of Q for the tensor-core sweep)
+        # and the update kernel; per check: the log-likelihood kernel and its final sum
         opt = EMAdamOptimizer(P.shape, Q.shape, HP["lr"], HP["beta1"], HP["beta2"], HP["eps"], dev, prec)
-        sweep_launches = 2 if prec in TC_PRECISIONS else 1
-        per_iter = sweep_launches + 1
-        step_stream = torch.cuda.Stream(device=dev, priority=-1)
-        side = torch.cuda.Stream(device=dev)
-        swept = {"v": False}
+        per_iter = 3 if prec in TC_PRECISIONS else 2
 
-        def one_step(it, last=False):
-            if not swept["v"]:
-                opt.sweep(G, P, Q, P32, Q32, M, ws)
-            swept["v"] = False
-            opt.update(P, Q, P32, Q32, M, ws)
+        def one_step(it):
+            opt.fused_iteration(G, P, Q, P32, Q32, M, ws)
             launches["n"] += per_iter
             if (it + 1) % CHECK == 0:
-                side.wait_stream(step_stream)
-                with torch.cuda.stream(side):
-                    out = ops.loglik_device(G, Pll, Qll, M, llp)
+                float(ops.loglik_device(G, Pll, Qll, M, llp).item())
                 launches["n"] += 2
-                if not last:
-                    opt.sweep(G, P, Q, P32, Q32, M, ws)
-                    swept["v"] = True
-                with torch.cuda.stream(side):
-                    float(out.item())
     else:
         # SNP-sharded: local sweep + statistics, all-reduce of T, targets, Adam (Q replicated)
         run = ShardedAdamEM(G, P, Q, M_loc, K, HP["beta1"], HP["beta2"], HP["eps"], HP["lr"],
                             backend=CudaBackend(prec))
         per_iter = (3 if prec in TC_PRECISIONS else 2) + 2
 
-        def one_step(it, last=False):
+        def one_step(it):
             run.iteration()
             launches["n"] += per_iter
             if (it + 1) % CHECK == 0:
@@ -307,9 +290,8 @@ def run_gpu_arm(args, cfg, rank, world, local_rank):
                 launches["n"] += 2
 
     torch.cuda.synchronize()
-    with torch.cuda.stream(step_stream):
-        for it in range(args.warmup):
-            one_step(it, last=it == args.warmup - 1)
+    for it in range(args.warmup):
+        one_step(it)
     torch.cuda.synchronize()
     launches["n"] = 0
     if sharded:
@@ -322,11 +304,11 @@ def run_gpu_arm(args, cfg, rank, world, local_rank):
         pass
     stream = torch.cuda.current_stream(dev)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with Clocks(uuid) as clk, torch.cuda.stream(step_stream):
-        e0.record(step_stream)
+    with Clocks(uuid) as clk:
+        e0.record(stream)
         for it in range(args.steps):
-            one_step(it, last=it == args.steps - 1)
-        e1.record(step_stream)
+            one_step(it)
+        e1.record(stream)
         torch.cuda.synchronize()
     ms = e0.elapsed_time(e1)
     if sharded:

@@ -136,15 +136,6 @@ int adx_em_adam_iteration(const uint8_t* G, int64_t M, int64_t N, int K, int pre
                           double* mQ, double* vQ, const double* q_bat, double t, double lr,
                           double beta1, double beta2, double eps, void* workspace,
                           size_t workspace_bytes, void* stream);
-/* The second launch of adx_em_adam_iteration alone, after adx_em_sweep filled the same
- * workspace (same shape and precision): statistics, EM targets and Adam move. With the
- * sweep and the move apart, a caller can run the log-likelihood check of the current P/Q
- * concurrently with the next sweep (both only read P/Q) -- the reference checks between
- * its iterations (em_adam_gpu.py:330-353). */
-int adx_em_adam_update(int64_t M, int64_t N, int K, int precision, double* P, double* Q,
-                       float* P32, float* Q32, double* mP, double* vP, double* mQ, double* vQ,
-                       const double* q_bat, double t, double lr, double beta1, double beta2,
-                       double eps, void* workspace, size_t workspace_bytes, void* stream);
 
 /* Binomial log-likelihood, float64 sum: sum over observed entries of
  * g log h + (2-g) log(1-h), h = clamp(P Q^T, 1e-10, 1-1e-10) (loglikelihood_gpu,

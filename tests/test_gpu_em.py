@@ -245,28 +245,6 @@ def test_loglik(ops, name, request):
     assert abs(l32 - ref) <= 1e-6 * abs(ref)
 
 
-@pytest.mark.parametrize("prec", ["f64", "f32", "f16", "mixed"])
-def test_overlapped_check_changes_nothing(ops, synth, prec):
-    # the log-likelihood check beside the next sweep (two streams) against the plain
-    # sequential loop: the same iterates, checks and returned fit, bit for bit
-    from adamixture_b200.model.em_adam_gpu import optimize_parameters_gpu
-
-    d = synth
-    M, N, K = int(d["M"]), int(d["N"]), int(d["K"])
-    G = dev_t(d["packed"])
-    out = {}
-    for ov in (False, True):
-        tr = []
-        P, Q = optimize_parameters_gpu(G, dev_t(d["P0"]), dev_t(d["Q0"]), 0.005, 0.80, 0.88, 1e-8, 10000, 5, K,
-                                       M, N, 0.5, 1e-4, 3, 0.1, G.device, 8192, 512, precision=prec, trace=tr,
-                                       overlap_check=ov)
-        torch.cuda.synchronize()
-        out[ov] = (P.cpu().numpy(), Q.cpu().numpy(), [(i, L) for i, L, _ in tr])
-    np.testing.assert_array_equal(out[True][0], out[False][0])
-    np.testing.assert_array_equal(out[True][1], out[False][1])
-    assert out[True][2] == out[False][2]
-
-
 @pytest.mark.parametrize("N,M,K", [(1024, 777, 10), (1026, 501, 8), (4000, 333, 3), (2048, 130, 16),
                                    (512, 64, 24), (1000, 97, 64)])
 def test_loglik_load_paths(ops, N, M, K):
