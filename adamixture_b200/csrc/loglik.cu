@@ -129,10 +129,13 @@ loglik_kernel(const uint8_t* __restrict__ G, const R* __restrict__ P, const R* _
       for (int qd = 0; qd < cn; qd += 4) {
         const uint32_t cur = word;
         if (qd + 4 < cn) word = load_word((c0 + qd + 4) >> 2);  // next quad, ahead of the math
+        // no early exit for a ragged chunk end (only the last chunk, when M % 4 != 0): the
+        // entries past it count as missing (factor 1), so the four SNPs' dot products are
+        // independent and interleave (Ps rows past cn are zeros, inside the CH-row tile)
 #pragma unroll
         for (int s = 0; s < 4; ++s) {
           const int jl = qd + s;
-          if (jl >= cn) break;
+          const bool live = jl < cn;
           R h[SPT];
           if constexpr (PAIRS) {
 #pragma unroll
@@ -155,7 +158,7 @@ loglik_kernel(const uint8_t* __restrict__ G, const R* __restrict__ P, const R* _
           }
 #pragma unroll
           for (int u = 0; u < SPT; ++u) {
-            const unsigned g = genotype(cur >> (8 * u), s);
+            const unsigned g = live ? genotype(cur >> (8 * u), s) : 3u;
             if constexpr (sizeof(R) == 4) {
               // float32 h: the factor in float32 as well (its rounding, 6e-8 relative, is below
               // that of h itself); the clamp h in [1e-10, 1-1e-10] is applied to h and to 1-h,
