@@ -18,7 +18,8 @@
 // walks a range of the other axis in chunks of 32: per chunk it stages the factor rows,
 // forms the 32 x 64 pair products and the 64 x 32 coefficients (h, then a/h and b/(1-h))
 // once in shared memory, and each thread accumulates a 4-row x 4-pair tile of the product
-// (register-tiled float64 FMAs). The gradient rides along in the CTAs of the first pair
+// (register-tiled float64 FMAs; its rows interleaved 16 apart so the warp's coefficient
+// reads are conflict-free). The gradient rides along in the CTAs of the first pair
 // block. Ranges of the reduced axis are split across CTAs when the row tiles alone do not
 // fill the GPU; their sums meet in float64 atomics on the zeroed outputs.
 #include "common.cuh"
@@ -175,14 +176,14 @@ __global__ void __launch_bounds__(TPB) grad_hess_kernel(Args a) {
     const int cmax = (int)min((int64_t)CJ, n_red - red0);
 #pragma unroll
     for (int t = 0; t < NT; ++t) {
-      const double* cf = s.coef + t * CJ * TR + rg * 4;
+      // the thread's rows are rg + 16 i: the 16 row groups of a warp read 16 consecutive
+      // coefficients (one conflict-free wavefront, the other half-warp a broadcast)
+      const double* cf = s.coef + t * CJ * TR + rg;
       const double* pr = s.pp + t * CJ * TP + pg * 4;
       for (int c = 0; c < cmax; ++c) {
-        const double2 a01 = *reinterpret_cast<const double2*>(cf + c * TR);
-        const double2 a23 = *reinterpret_cast<const double2*>(cf + c * TR + 2);
         const double2 b01 = *reinterpret_cast<const double2*>(pr + c * TP);
         const double2 b23 = *reinterpret_cast<const double2*>(pr + c * TP + 2);
-        const double av[4] = {a01.x, a01.y, a23.x, a23.y};
+        const double av[4] = {cf[c * TR], cf[c * TR + 16], cf[c * TR + 32], cf[c * TR + 48]};
         const double bv[4] = {b01.x, b01.y, b23.x, b23.y};
 #pragma unroll
         for (int i = 0; i < 4; ++i)
@@ -207,7 +208,7 @@ __global__ void __launch_bounds__(TPB) grad_hess_kernel(Args a) {
   // scatter: both halves of the symmetric Hessian
 #pragma unroll
   for (int i = 0; i < 4; ++i) {
-    const int64_t row = row0 + rg * 4 + i;
+    const int64_t row = row0 + rg + 16 * i;
     if (row >= n_rows) continue;
     double* H = a.XtX + row * K * K;
 #pragma unroll
