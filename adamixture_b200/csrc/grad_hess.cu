@@ -64,8 +64,12 @@ struct Smem {
   }
 };
 
-template <bool QSIDE>
+// KM: an upper bound of K known at compile time (4, 8, 12, 16, or 64 for the rest), which
+// sizes the gradient's per-thread registers and loops: thread (row gr, k = gk0 + 4 m) for
+// m < KM / 4 instead of issuing predicated-off iterations up to K = 64.
+template <bool QSIDE, int KM>
 __global__ void __launch_bounds__(TPB) grad_hess_kernel(Args a) {
+  constexpr int MG = KM / 4;   // gradient entries per thread
   constexpr int NT = QSIDE ? 2 : 1;   // coefficient terms
   extern __shared__ __align__(16) uint8_t smem[];
   const int K = a.K;
@@ -107,10 +111,10 @@ __global__ void __launch_bounds__(TPB) grad_hess_kernel(Args a) {
   for (int i = 0; i < 4; ++i)
 #pragma unroll
     for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
-  // gradient: thread (row r = tid & 63, k = (tid >> 6) + 4 m), m < 16
-  double xz[16];
+  // gradient: thread (row r = tid & 63, k = (tid >> 6) + 4 m), m < MG
+  double xz[MG];
 #pragma unroll
-  for (int m = 0; m < 16; ++m) xz[m] = 0.0;
+  for (int m = 0; m < MG; ++m) xz[m] = 0.0;
   const int gr = tid & (TR - 1), gk0 = tid >> 6;
 
   const int64_t n_chunks = (n_red + CJ - 1) / CJ;
@@ -197,7 +201,7 @@ __global__ void __launch_bounds__(TPB) grad_hess_kernel(Args a) {
         const double y1 = s.zc[c * TR + gr];
         const double y2 = QSIDE ? s.zc[CJ * TR + c * TR + gr] : 0.0;
 #pragma unroll
-        for (int m = 0; m < 16; ++m) {
+        for (int m = 0; m < MG; ++m) {
           const int k = gk0 + 4 * m;
           if (k < K) xz[m] += QSIDE ? (y1 * f[k] + y2 * (1.0 - f[k])) : (y1 * f[k]);
         }
@@ -225,7 +229,7 @@ __global__ void __launch_bounds__(TPB) grad_hess_kernel(Args a) {
     const int64_t row = row0 + gr;
     if (row < n_rows) {
 #pragma unroll
-      for (int m = 0; m < 16; ++m) {
+      for (int m = 0; m < MG; ++m) {
         const int k = gk0 + 4 * m;
         if (k < K) atomicAdd(a.Xtz + row * K + k, xz[m]);
       }
@@ -237,6 +241,14 @@ __global__ void __launch_bounds__(TPB) grad_hess_kernel(Args a) {
 }  // namespace adx
 
 using namespace adx;
+
+template <bool QSIDE, int KM>
+static int grad_hess_launch(const gh::Args& a, size_t smem, int64_t blocks, cudaStream_t st) {
+  ADX_CUDA_TRY(cudaFuncSetAttribute(gh::grad_hess_kernel<QSIDE, KM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  gh::grad_hess_kernel<QSIDE, KM><<<(unsigned)blocks, gh::TPB, smem, st>>>(a);
+  ADX_LAUNCH_CHECK();
+  return ADX_OK;
+}
 
 template <bool QSIDE>
 static int grad_hess(const uint8_t* G, int64_t M, int64_t N, int K, const double* P, const double* Q,
@@ -260,11 +272,12 @@ static int grad_hess(const uint8_t* G, int64_t M, int64_t N, int K, const double
   a.chunks_per_split = ceil_div(n_chunks, split);
   a.n_split = (int)ceil_div(n_chunks, a.chunks_per_split);
   const size_t smem = gh::Smem::bytes(K, QSIDE ? 2 : 1);
-  ADX_CUDA_TRY(cudaFuncSetAttribute(gh::grad_hess_kernel<QSIDE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   const int64_t blocks = tiles * a.n_pblk * a.n_split;
-  gh::grad_hess_kernel<QSIDE><<<(unsigned)blocks, gh::TPB, smem, st>>>(a);
-  ADX_LAUNCH_CHECK();
-  return ADX_OK;
+  if (K <= 4) return grad_hess_launch<QSIDE, 4>(a, smem, blocks, st);
+  if (K <= 8) return grad_hess_launch<QSIDE, 8>(a, smem, blocks, st);
+  if (K <= 12) return grad_hess_launch<QSIDE, 12>(a, smem, blocks, st);
+  if (K <= 16) return grad_hess_launch<QSIDE, 16>(a, smem, blocks, st);
+  return grad_hess_launch<QSIDE, 64>(a, smem, blocks, st);
 }
 
 extern "C" int adx_grad_hess_q(const uint8_t* G, int64_t M, int64_t N, int K, const double* P, const double* Q,
