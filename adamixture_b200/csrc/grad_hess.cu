@@ -64,12 +64,13 @@ struct Smem {
   }
 };
 
-// KM: an upper bound of K known at compile time (4, 8, 12, 16, or 64 for the rest), which
-// sizes the gradient's per-thread registers and loops: thread (row gr, k = gk0 + 4 m) for
-// m < KM / 4 instead of issuing predicated-off iterations up to K = 64.
+// KM: an upper bound of K known at compile time (4, 6, 8, 10, 12, 16, or 64 for the rest),
+// which sizes the gradient's per-thread registers and loops -- thread (row gr,
+// k = gk0 + 4 m) for m < ceil(KM / 4) instead of issuing predicated-off iterations up to
+// K = 64 -- and, for KM <= 16, the factor row kept in registers.
 template <bool QSIDE, int KM>
 __global__ void __launch_bounds__(TPB) grad_hess_kernel(Args a) {
-  constexpr int MG = KM / 4;   // gradient entries per thread
+  constexpr int MG = (KM + 3) / 4;   // gradient entries per thread
   constexpr int NT = QSIDE ? 2 : 1;   // coefficient terms
   extern __shared__ __align__(16) uint8_t smem[];
   const int K = a.K;
@@ -143,7 +144,15 @@ __global__ void __launch_bounds__(TPB) grad_hess_kernel(Args a) {
       s.pp[c * TP + t] = v0;
       if (QSIDE) s.pp[CJ * TP + c * TP + t] = v1;
     }
-    // coefficients of the TR x CJ entries; lanes walk the sample axis of G
+    // coefficients of the TR x CJ entries; lanes walk the sample axis of G. A thread's
+    // entries share one factor row -- its row (tid & 63) on the Q side, its reduced entry
+    // (tid & 31) on the P side -- held in registers for K <= 16
+    double fix[KM <= 16 ? KM : 1];
+    if constexpr (KM <= 16) {
+      const double* src = QSIDE ? s.own + (tid & (TR - 1)) * K : s.fac + (tid & (CJ - 1)) * K;
+#pragma unroll
+      for (int k = 0; k < KM; ++k) fix[k] = k < K ? src[k] : 0.0;
+    }
     for (int e = tid; e < TR * CJ; e += TPB) {
       int r, c;
       if (QSIDE) { c = e / TR; r = e - c * TR; } else { r = e / CJ; c = e - r * CJ; }
@@ -154,7 +163,14 @@ __global__ void __launch_bounds__(TPB) grad_hess_kernel(Args a) {
         const unsigned g = genotype(a.G[(snp >> 2) * a.N + smp], (int)(snp & 3));
         if (g != 3u) {
           double h = 0.0;
-          for (int k = 0; k < K; ++k) h += s.own[r * K + k] * s.fac[c * K + k];
+          if constexpr (KM <= 16) {
+            const double* var = QSIDE ? s.fac + c * K : s.own + r * K;
+#pragma unroll
+            for (int k = 0; k < KM; ++k)
+              if (k < K) h += QSIDE ? fix[k] * var[k] : var[k] * fix[k];
+          } else {
+            for (int k = 0; k < K; ++k) h += s.own[r * K + k] * s.fac[c * K + k];
+          }
           h = fmax(fmin(h, 1.0 - 1e-10), 1e-10);
           const double gd = (double)g, om = 1.0 - h;
           // one division: 1/h and 1/(1-h) from 1/(h(1-h))
@@ -274,7 +290,9 @@ static int grad_hess(const uint8_t* G, int64_t M, int64_t N, int K, const double
   const size_t smem = gh::Smem::bytes(K, QSIDE ? 2 : 1);
   const int64_t blocks = tiles * a.n_pblk * a.n_split;
   if (K <= 4) return grad_hess_launch<QSIDE, 4>(a, smem, blocks, st);
+  if (K <= 6) return grad_hess_launch<QSIDE, 6>(a, smem, blocks, st);
   if (K <= 8) return grad_hess_launch<QSIDE, 8>(a, smem, blocks, st);
+  if (K <= 10) return grad_hess_launch<QSIDE, 10>(a, smem, blocks, st);
   if (K <= 12) return grad_hess_launch<QSIDE, 12>(a, smem, blocks, st);
   if (K <= 16) return grad_hess_launch<QSIDE, 16>(a, smem, blocks, st);
   return grad_hess_launch<QSIDE, 64>(a, smem, blocks, st);

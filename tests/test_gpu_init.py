@@ -71,6 +71,23 @@ def test_grad_hess_vs_reference(ops, solvers_golden, tag):
         np.testing.assert_allclose(got.cpu().numpy(), ref, rtol=1e-9, atol=1e-9 * np.abs(ref).max())
 
 
+@pytest.mark.parametrize("K", [7, 8, 10, 16, 20, 64])
+def test_grad_hess_every_k_bound(ops, K):
+    # every compile-time bound of K (exact 10, 8 and 16, 64 for the rest) against the float64
+    # restatement; several row tiles, reduced-axis chunks and, for K = 64, pair blocks
+    rng = np.random.default_rng(K)
+    M, N = 333, 150
+    G = rng.choice(4, size=(M, N), p=[0.3, 0.35, 0.3, 0.05]).astype(np.uint8)
+    P = np.clip(rng.beta(0.8, 0.8, size=(M, K)), 1e-5, 1 - 1e-5)
+    Q = rng.dirichlet(np.full(K, 0.5), size=N)
+    Gp = dev(orc.pack(G))
+    out = {"q": ops.grad_hess_q(Gp, dev(P), dev(Q), M), "p": ops.grad_hess_p(Gp, dev(P), dev(Q), M)}
+    ref = {"q": osv.grad_hess_q(G, P, Q), "p": osv.grad_hess_p(G, P, Q)}
+    for side in ("q", "p"):
+        for got, want in zip(out[side], ref[side]):
+            np.testing.assert_allclose(got.cpu().numpy(), want, rtol=1e-9, atol=1e-9 * np.abs(want).max())
+
+
 @pytest.mark.parametrize("tag", ["a", "b", "c"])
 def test_sqp_vs_reference(ops, solvers_golden, tag):
     d = solvers_golden
