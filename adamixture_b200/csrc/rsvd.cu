@@ -10,83 +10,95 @@
 // shared memory and contracts them on the spot, so the only HBM traffic is the packed
 // genotypes (0.25 B per entry) and the factors.
 //
-// Both kernels: 256 threads = 32 groups of 4 "own" indices (SNPs for rows, samples for
-// cols) x 8 groups of LP/8 factor columns; each thread keeps a 4 x LP/8 float32 tile of
-// the output in registers and walks the contracted axis in chunks staged in shared memory
-// (factor rows of the chunk, decoded genotype block). L <= 80 (LP = L rounded up to 8).
-// Partial sums of the cols product over SNP ranges go to a workspace and are added in a
-// fixed order, so results do not depend on scheduling.
+// Both kernels: 256 threads = 64 groups of OP "own" indices (SNPs for rows, samples for
+// cols; OP = 8 while L <= 32, else 4) x 4 groups of C = LP/4 factor columns; each thread
+// keeps an OP x C float32 tile of the output in registers and walks the contracted axis in
+// chunks staged in shared memory (factor rows of the chunk, decoded genotype block of 32 KB).
+// A thread's own indices are OP/4 runs of 4 spaced 256 apart, so each 16-byte load of the
+// decoded block covers 512 contiguous bytes across the warp (no bank conflicts); shared
+// loads per FMA are about 1/C + 1/OP. L <= 80 (LP = L rounded up to 4). Partial sums of the
+// cols product over SNP ranges go to a workspace and are added in a fixed order, so
+// results do not depend on scheduling.
 #include "common.cuh"
 
 namespace adx {
 namespace rsvd {
 
 constexpr int TPB = 256;
-constexpr int OWN = 128;      // own indices per CTA (32 groups of 4)
-constexpr int CH = 32;        // contracted indices per chunk
+constexpr int OG = 64;        // own groups
+constexpr int CG = 4;         // column groups
+constexpr int CH = 32;        // granularity of the cols product's SNP ranges
 constexpr int LMAX = 80;
-constexpr int CG = 8;         // column groups
+constexpr int XS_FLOATS = 8192;  // decoded block: 32 KB
+
+// own indices per thread for C columns per thread
+__host__ __device__ constexpr int own_per_thread(int C) { return C <= 8 ? 8 : 4; }
 
 __device__ __forceinline__ float centred(uint32_t byte, int s, float two_f) {
   const uint32_t g = (byte >> (2 * s)) & 3u;
   return g == 3u ? 0.0f : (float)g - two_f;
 }
 
-// Y[j][:] = sum_i Xc[j][i] B[i][:] for the 128 SNPs of this CTA.
-template <int C>  // columns per thread group = LP / 8
+// own index of (thread group og, run v, slot q)
+__device__ __forceinline__ int own_of(int og, int v, int q) { return v * (OG * 4) + og * 4 + q; }
+
+// Y[j][:] = sum_i Xc[j][i] B[i][:] for the OWN SNPs of this CTA.
+template <int C>  // columns per thread = LP / 4
 __global__ void __launch_bounds__(TPB) rows_kernel(const uint8_t* __restrict__ G, int64_t M, int64_t N,
                                                    const float* __restrict__ f, const float* __restrict__ B,
                                                    int L, float* __restrict__ Y) {
-  constexpr int LP = C * CG;
-  __shared__ __align__(16) float xs[CH][OWN];   // [sample][snp]
-  __shared__ __align__(16) float bs[CH][LP];
+  constexpr int LP = C * CG, OP = own_per_thread(C), OWN = OG * OP, CHK = XS_FLOATS / OWN;
+  __shared__ __align__(16) float xs[CHK][OWN];   // [sample][snp]
+  __shared__ __align__(16) float bs[CHK][LP];
   __shared__ float tf[OWN];
-  const int tid = threadIdx.x, og = tid & 31, cg = tid >> 5;
+  const int tid = threadIdx.x, og = tid & (OG - 1), cg = tid / OG;
   const int64_t j0 = (int64_t)blockIdx.x * OWN;
   for (int t = tid; t < OWN; t += TPB) {
     const int64_t j = j0 + t;
     tf[t] = j < M ? 2.0f * f[j] : 0.0f;
   }
-  float acc[4][C];
+  float acc[OP][C];
 #pragma unroll
-  for (int a = 0; a < 4; ++a)
+  for (int a = 0; a < OP; ++a)
 #pragma unroll
     for (int c = 0; c < C; ++c) acc[a][c] = 0.0f;
   const int64_t rows = (M + 3) >> 2;
-  for (int64_t i0 = 0; i0 < N; i0 += CH) {
+  for (int64_t i0 = 0; i0 < N; i0 += CHK) {
     __syncthreads();
-    for (int e = tid; e < CH * LP; e += TPB) {
+    for (int e = tid; e < CHK * LP; e += TPB) {
       const int s = e / LP, l = e - s * LP;
       const int64_t i = i0 + s;
       bs[s][l] = (i < N && l < L) ? B[i * L + l] : 0.0f;
     }
-    // 32 packed rows x 32 samples: one byte gives 4 SNPs of one sample
-    for (int e = tid; e < (OWN / 4) * CH; e += TPB) {
-      const int pr = e / CH, s = e - pr * CH;
+    // OWN/4 packed rows x CHK samples: one byte gives 4 SNPs of one sample
+    for (int e = tid; e < (OWN / 4) * CHK; e += TPB) {
+      const int pr = e / CHK, s = e - pr * CHK;
       const int64_t row = (j0 >> 2) + pr, i = i0 + s;
       const uint32_t byte = (row < rows && i < N) ? (uint32_t)G[row * N + i] : 0xFFu;
 #pragma unroll
       for (int q = 0; q < 4; ++q) xs[s][pr * 4 + q] = centred(byte, q, tf[pr * 4 + q]);
     }
     __syncthreads();
-    const int smax = (int)min((int64_t)CH, N - i0);
+    const int smax = (int)min((int64_t)CHK, N - i0);
     for (int s = 0; s < smax; ++s) {
-      const float4 x = *reinterpret_cast<const float4*>(&xs[s][og * 4]);
+      float x[OP];
+#pragma unroll
+      for (int v = 0; v < OP / 4; ++v) {
+        const float4 x4 = *reinterpret_cast<const float4*>(&xs[s][own_of(og, v, 0)]);
+        x[4 * v] = x4.x; x[4 * v + 1] = x4.y; x[4 * v + 2] = x4.z; x[4 * v + 3] = x4.w;
+      }
       float b[C];
 #pragma unroll
       for (int c = 0; c < C; ++c) b[c] = bs[s][cg * C + c];
 #pragma unroll
-      for (int c = 0; c < C; ++c) {
-        acc[0][c] = fmaf(x.x, b[c], acc[0][c]);
-        acc[1][c] = fmaf(x.y, b[c], acc[1][c]);
-        acc[2][c] = fmaf(x.z, b[c], acc[2][c]);
-        acc[3][c] = fmaf(x.w, b[c], acc[3][c]);
-      }
+      for (int a = 0; a < OP; ++a)
+#pragma unroll
+        for (int c = 0; c < C; ++c) acc[a][c] = fmaf(x[a], b[c], acc[a][c]);
     }
   }
 #pragma unroll
-  for (int a = 0; a < 4; ++a) {
-    const int64_t j = j0 + og * 4 + a;
+  for (int a = 0; a < OP; ++a) {
+    const int64_t j = j0 + own_of(og, a >> 2, a & 3);
     if (j >= M) continue;
 #pragma unroll
     for (int c = 0; c < C; ++c) {
@@ -96,41 +108,42 @@ __global__ void __launch_bounds__(TPB) rows_kernel(const uint8_t* __restrict__ G
   }
 }
 
-// Partial Z over one SNP range for the 128 samples of this CTA: part[split][i][:].
+// Partial Z over one SNP range for the OWN samples of this CTA: part[split][i][:].
 template <int C>
 __global__ void __launch_bounds__(TPB) cols_kernel(const uint8_t* __restrict__ G, int64_t M, int64_t N,
                                                    const float* __restrict__ f, const float* __restrict__ Yf,
                                                    int L, int64_t snps_per_split, float* __restrict__ part) {
-  constexpr int LP = C * CG;
-  __shared__ __align__(16) float xs[CH][OWN];   // [snp][sample]
-  __shared__ __align__(16) float ys[CH][LP];
-  __shared__ float tf[CH];
-  const int tid = threadIdx.x, og = tid & 31, cg = tid >> 5;
+  constexpr int LP = C * CG, OP = own_per_thread(C), OWN = OG * OP, CHK = XS_FLOATS / OWN;
+  static_assert(CHK % 4 == 0 && CH % CHK == 0, "SNP chunks are whole packed rows inside a range");
+  __shared__ __align__(16) float xs[CHK][OWN];   // [snp][sample]
+  __shared__ __align__(16) float ys[CHK][LP];
+  __shared__ float tf[CHK];
+  const int tid = threadIdx.x, og = tid & (OG - 1), cg = tid / OG;
   const int64_t n_tiles = (N + OWN - 1) / OWN;
   const int64_t tile = blockIdx.x % n_tiles;
   const int split = (int)(blockIdx.x / n_tiles);
   const int64_t i0 = tile * OWN;
   const int64_t js = (int64_t)split * snps_per_split;
   const int64_t je = min(M, js + snps_per_split);
-  float acc[4][C];
+  float acc[OP][C];
 #pragma unroll
-  for (int a = 0; a < 4; ++a)
+  for (int a = 0; a < OP; ++a)
 #pragma unroll
     for (int c = 0; c < C; ++c) acc[a][c] = 0.0f;
-  for (int64_t j0 = js; j0 < je; j0 += CH) {
+  for (int64_t j0 = js; j0 < je; j0 += CHK) {
     __syncthreads();
-    for (int e = tid; e < CH * LP; e += TPB) {
+    for (int e = tid; e < CHK * LP; e += TPB) {
       const int s = e / LP, l = e - s * LP;
       const int64_t j = j0 + s;
       ys[s][l] = (j < je && l < L) ? Yf[j * L + l] : 0.0f;
     }
-    if (tid < CH) {
+    if (tid < CHK) {
       const int64_t j = j0 + tid;
       tf[tid] = j < je ? 2.0f * f[j] : 0.0f;
     }
     __syncthreads();
-    // CH SNPs (CH/4 packed rows; js is a multiple of 4) x 128 samples
-    for (int e = tid; e < (CH / 4) * OWN; e += TPB) {
+    // CHK SNPs (CHK/4 packed rows; js is a multiple of 4) x OWN samples
+    for (int e = tid; e < (CHK / 4) * OWN; e += TPB) {
       const int pr = e / OWN, s = e - pr * OWN;
       const int64_t row = (j0 >> 2) + pr, i = i0 + s;
       const uint32_t byte = (j0 + pr * 4 < je && i < N) ? (uint32_t)G[row * N + i] : 0xFFu;
@@ -141,25 +154,27 @@ __global__ void __launch_bounds__(TPB) cols_kernel(const uint8_t* __restrict__ G
       }
     }
     __syncthreads();
-    const int jmax = (int)min((int64_t)CH, je - j0);
+    const int jmax = (int)min((int64_t)CHK, je - j0);
     for (int s = 0; s < jmax; ++s) {
-      const float4 x = *reinterpret_cast<const float4*>(&xs[s][og * 4]);
+      float x[OP];
+#pragma unroll
+      for (int v = 0; v < OP / 4; ++v) {
+        const float4 x4 = *reinterpret_cast<const float4*>(&xs[s][own_of(og, v, 0)]);
+        x[4 * v] = x4.x; x[4 * v + 1] = x4.y; x[4 * v + 2] = x4.z; x[4 * v + 3] = x4.w;
+      }
       float y[C];
 #pragma unroll
       for (int c = 0; c < C; ++c) y[c] = ys[s][cg * C + c];
 #pragma unroll
-      for (int c = 0; c < C; ++c) {
-        acc[0][c] = fmaf(x.x, y[c], acc[0][c]);
-        acc[1][c] = fmaf(x.y, y[c], acc[1][c]);
-        acc[2][c] = fmaf(x.z, y[c], acc[2][c]);
-        acc[3][c] = fmaf(x.w, y[c], acc[3][c]);
-      }
+      for (int a = 0; a < OP; ++a)
+#pragma unroll
+        for (int c = 0; c < C; ++c) acc[a][c] = fmaf(x[a], y[c], acc[a][c]);
     }
   }
   float* out = part + (int64_t)split * N * L;
 #pragma unroll
-  for (int a = 0; a < 4; ++a) {
-    const int64_t i = i0 + og * 4 + a;
+  for (int a = 0; a < OP; ++a) {
+    const int64_t i = i0 + own_of(og, a >> 2, a & 3);
     if (i >= N) continue;
 #pragma unroll
     for (int c = 0; c < C; ++c) {
@@ -187,7 +202,8 @@ struct ColsPlan {
 
 static ColsPlan cols_plan(int64_t M, int64_t N, int L) {
   ColsPlan p{};
-  const int64_t tiles = ceil_div(N, OWN);
+  const int C = (L + CG - 1) / CG;
+  const int64_t tiles = ceil_div(N, (int64_t)OG * own_per_thread(C));
   // enough CTAs for about 4 per SM; SNP ranges are whole chunks
   int64_t split = ceil_div((int64_t)sm_count() * 4, tiles);
   const int64_t chunks = ceil_div(M, CH);
@@ -203,11 +219,13 @@ static ColsPlan cols_plan(int64_t M, int64_t N, int L) {
 
 using namespace adx;
 
-#define ADX_LP_SWITCH(L, X)                                                         \
-  switch ((L + 7) / 8) {                                                            \
-    case 1: X(1) break; case 2: X(2) break; case 3: X(3) break; case 4: X(4) break; \
-    case 5: X(5) break; case 6: X(6) break; case 7: X(7) break; case 8: X(8) break; \
-    case 9: X(9) break; default: X(10) break;                                       \
+#define ADX_LP_SWITCH(L, X)                                                              \
+  switch ((L + 3) / 4) {                                                                 \
+    case 1: X(1) break;   case 2: X(2) break;   case 3: X(3) break;   case 4: X(4) break;   \
+    case 5: X(5) break;   case 6: X(6) break;   case 7: X(7) break;   case 8: X(8) break;   \
+    case 9: X(9) break;   case 10: X(10) break; case 11: X(11) break; case 12: X(12) break; \
+    case 13: X(13) break; case 14: X(14) break; case 15: X(15) break; case 16: X(16) break; \
+    case 17: X(17) break; case 18: X(18) break; case 19: X(19) break; default: X(20) break; \
   }
 
 extern "C" int adx_rsvd_workspace_bytes(int64_t M, int64_t N, int L, size_t* bytes) {
@@ -226,7 +244,8 @@ extern "C" int adx_rsvd_rows(const uint8_t* G, int64_t M, int64_t N, const float
     return ADX_ERR_ARG;
   }
   cudaStream_t st = as_stream(stream);
-  const unsigned blocks = (unsigned)ceil_div(M, rsvd::OWN);
+  const int64_t own = (int64_t)rsvd::OG * rsvd::own_per_thread((L + rsvd::CG - 1) / rsvd::CG);
+  const unsigned blocks = (unsigned)ceil_div(M, own);
 #define LAUNCH(C) rsvd::rows_kernel<C><<<blocks, rsvd::TPB, 0, st>>>(G, M, N, f, B, L, Y);
   ADX_LP_SWITCH(L, LAUNCH)
 #undef LAUNCH
@@ -247,7 +266,8 @@ extern "C" int adx_rsvd_cols(const uint8_t* G, int64_t M, int64_t N, const float
   }
   cudaStream_t st = as_stream(stream);
   float* part = static_cast<float*>(workspace);
-  const unsigned blocks = (unsigned)(ceil_div(N, rsvd::OWN) * p.n_split);
+  const int64_t own = (int64_t)rsvd::OG * rsvd::own_per_thread((L + rsvd::CG - 1) / rsvd::CG);
+  const unsigned blocks = (unsigned)(ceil_div(N, own) * p.n_split);
 #define LAUNCH(C) rsvd::cols_kernel<C><<<blocks, rsvd::TPB, 0, st>>>(G, M, N, f, Y, L, p.snps_per_split, part);
   ADX_LP_SWITCH(L, LAUNCH)
 #undef LAUNCH

@@ -34,7 +34,8 @@ def ops(cuda):
     return _ops
 
 
-@pytest.mark.parametrize("N,M,L", [(23, 37, 5), (300, 1001, 20), (1000, 257, 17), (129, 4099, 80)])
+@pytest.mark.parametrize("N,M,L", [(23, 37, 5), (300, 1001, 20), (1000, 257, 17), (129, 4099, 80),
+                                   (2000, 3001, 32), (700, 1500, 33), (64, 5000, 12)])
 def test_rsvd_products(ops, N, M, L):
     rng = np.random.default_rng(N + M + L)
     G = rng.choice(4, size=(M, N), p=[0.3, 0.35, 0.3, 0.05]).astype(np.uint8)
