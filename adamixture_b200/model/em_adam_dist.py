@@ -66,9 +66,14 @@ class CudaBackend:
         ops.adam_step(P, Q, P_EM, Q_EM, st["mP"], st["vP"], st["mQ"], st["vQ"], t, lr, beta1, beta2, eps)
 
     def loglik(self, G, P, Q, M):
+        """As the single-GPU optimiser's check: h in float64 for the float64 E-step, in
+        float32 otherwise (the sum stays float64)."""
         from .. import ops
+        from .em_adam_gpu import resolve_precision
 
-        return ops.loglik_device(G, P, Q, M, "f64")
+        if resolve_precision(Q.shape[1], self.precision) == "f64":
+            return ops.loglik_device(G, P, Q, M, "f64")
+        return ops.loglik_device(G, P.float().contiguous(), Q.float().contiguous(), M, "f32")
 
 
 class ShardedAdamEM:
