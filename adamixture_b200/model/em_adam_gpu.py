@@ -175,7 +175,7 @@ def _optimize_parameters_gpu_once(G, P, Q, lr, beta1, beta2, reg_adam, max_iter,
     ``check`` iterations. The reference's second priming E-step, whose result it never
     uses (:322), is skipped: it changes no state. ``trace`` (a list) receives
     ``(iteration, loglik, seconds since the start)`` at each check (host clock after the
-    check's read-back, so the device work up to it is included). ``precision="mixed"``: tensor-core (BF16) sweeps
+    check's read-back, so the device work up to it is included). ``precision="mixed"``: tensor-core sweeps
     until the first plateau (``patience`` checks without a new best), float32 sweeps after
     it, with the same Adam state and learning rate.
     """
@@ -222,11 +222,11 @@ def _optimize_parameters_gpu_once(G, P, Q, lr, beta1, beta2, reg_adam, max_iter,
             else:
                 wait_lr += 1
                 if wait_lr >= patience and mixed and prec != "f32":
-                    # mixed precision: the first plateau ends the BF16 phase; the same Adam
+                    # mixed precision: the first plateau ends the tensor-core phase; the same Adam
                     # state continues with float32 sweeps (same float32 P/Q shadows)
                     prec = opt.precision = "f32"
                     ws = ops.Workspace.get(G.device, ops.em_workspace_bytes(M, N, K, prec))
-                    log.info("    Plateau in the BF16 phase: continuing with float32 E-steps.")
+                    log.info("    Plateau in the tensor-core phase: continuing with float32 E-steps.")
                     wait_lr = 0
                     continue
                 if wait_lr >= patience:

@@ -566,9 +566,10 @@ def run_kernels(args, cfg):
 
 def run_converge(args, cfg):
     """Time to the converged log-likelihood at the config: from the reference's default
-    start (randomized SVD + ALS), plain float32 Adam-EM to its stop, then BF16, mixed
-    (BF16 then float32) and the learned warm start + mixed, each timed to the first check
-    within 1e-6 relative of the plain float32 run's best log-likelihood. One JSON line."""
+    start (randomized SVD + ALS), plain float32 Adam-EM to its stop, then the BF16 and FP16
+    tensor-core sweeps, mixed (tensor-core then float32) and the learned warm start with
+    the default arithmetic, each timed to the first check within 1e-6 relative of the plain
+    float32 run's best log-likelihood. One JSON line."""
     import torch
 
     from adamixture_b200 import ops
