@@ -17,9 +17,12 @@
 // on the row. A CTA owns 64 rows and 64 (k <= l) pairs of the symmetric K x K Hessian and
 // walks a range of the other axis in chunks of 32: per chunk it stages the factor rows,
 // forms the 32 x 64 pair products and the 64 x 32 coefficients (h, then a/h and b/(1-h))
-// once in shared memory, and each thread accumulates a 4-row x 4-pair tile of the product
-// (register-tiled float64 FMAs; its rows interleaved 16 apart so the warp's coefficient
-// reads are conflict-free). The gradient rides along in the CTAs of the first pair
+// once in shared memory, and the product runs on the float64 tensor-core MMA
+// (mma.sync m16n8k4 .f64: 512 FMAs per warp instruction, operands from registers): each
+// warp owns 32 rows x 16 pairs as 2 x 2 MMA tiles, loading its fragments from shared
+// memory whose rows are padded by 4 doubles so a fragment load is conflict-free. Every
+// chunk enters the MMAs whole: entries past the reduced axis have zero coefficients. The
+// gradient rides along in the CTAs of the first pair
 // block. Ranges of the reduced axis are split across CTAs when the row tiles alone do not
 // fill the GPU; their sums meet in float64 atomics on the zeroed outputs.
 #include "common.cuh"
@@ -30,7 +33,9 @@ namespace gh {
 constexpr int TR = 64;       // rows per tile
 constexpr int TP = 64;       // pairs per tile
 constexpr int CJ = 32;       // reduced-axis entries per chunk
-constexpr int TPB = 256;     // 16 row groups x 16 pair groups, 4 x 4 each
+constexpr int TPB = 256;     // 8 warps: 2 row blocks of 32 x 4 pair blocks of 16
+constexpr int CSTR = TR + 4; // padded row stride of the coefficient tiles (doubles)
+constexpr int PSTR = TP + 4; // padded row stride of the pair-product tiles (doubles)
 
 struct Args {
   const uint8_t* G;
@@ -45,20 +50,29 @@ struct Args {
   int64_t chunks_per_split;
 };
 
+// d (4 doubles: rows g, g, g+8, g+8; columns 2t, 2t+1, 2t, 2t+1 of a 16 x 8 tile) +=
+// A (16 x 4: a0 row g, a1 row g+8, column t) . B (4 x 8: b0 row t, column g), float64
+// tensor-core MMA; g = lane / 4, t = lane % 4.
+__device__ __forceinline__ void mma_f64(double (&d)[4], double a0, double a1, double b0) {
+  asm volatile("mma.sync.aligned.m16n8k4.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5}, {%6}, {%0,%1,%2,%3};"
+               : "+d"(d[0]), "+d"(d[1]), "+d"(d[2]), "+d"(d[3])
+               : "d"(a0), "d"(a1), "d"(b0));
+}
+
 // shared-memory layout (doubles unless noted)
 struct Smem {
   double *own, *fac, *coef, *zc, *pp;
   uint8_t *pk, *pl;
   static __host__ size_t bytes(int K, int nt) {
-    return sizeof(double) * ((size_t)(TR + CJ) * K + (size_t)nt * CJ * TR * 2 + (size_t)nt * CJ * TP) + 2 * TP;
+    return sizeof(double) * ((size_t)(TR + CJ) * K + (size_t)nt * CJ * (CSTR + TR) + (size_t)nt * CJ * PSTR) + 2 * TP;
   }
   __device__ Smem(uint8_t* base, int K, int nt) {
     double* d = reinterpret_cast<double*>(base);
     own = d; d += TR * K;            // [TR][K] factors of the tile's rows
     fac = d; d += CJ * K;            // [CJ][K] factors of the chunk's reduced entries
-    coef = d; d += nt * CJ * TR;     // [nt][CJ][TR] Hessian coefficients
+    coef = d; d += nt * CJ * CSTR;   // [nt][CJ][CSTR] Hessian coefficients
     zc = d; d += nt * CJ * TR;       // [nt][CJ][TR] gradient coefficients
-    pp = d; d += nt * CJ * TP;       // [nt][CJ][TP] pair products
+    pp = d; d += nt * CJ * PSTR;     // [nt][CJ][PSTR] pair products
     pk = reinterpret_cast<uint8_t*>(d);
     pl = pk + TP;
   }
@@ -76,7 +90,9 @@ __global__ void __launch_bounds__(TPB) grad_hess_kernel(Args a) {
   const int K = a.K;
   Smem s(smem, K, NT);
   const int tid = threadIdx.x;
-  const int rg = tid & 15, pg = tid >> 4;   // row group, pair group
+  const int lane = tid & 31, warp = tid >> 5;
+  const int fg = lane >> 2, ft = lane & 3;   // MMA fragment group and thread in group
+  const int wr = warp & 1, wp = warp >> 1;   // the warp's row block (32) and pair block (16)
   const int64_t n_rows = QSIDE ? a.N : a.M;
   const int64_t n_red = QSIDE ? a.M : a.N;
   const double* ownF = QSIDE ? a.Q : a.P;
@@ -107,11 +123,13 @@ __global__ void __launch_bounds__(TPB) grad_hess_kernel(Args a) {
     s.own[e] = row < n_rows ? ownF[row * K + k] : 0.0;
   }
 
-  double acc[4][4];
+  double acc[2][2][4];   // [row tile][pair tile][fragment]
 #pragma unroll
-  for (int i = 0; i < 4; ++i)
+  for (int i = 0; i < 2; ++i)
 #pragma unroll
-    for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
+    for (int j = 0; j < 2; ++j)
+#pragma unroll
+      for (int v = 0; v < 4; ++v) acc[i][j][v] = 0.0;
   // gradient: thread (row r = tid & 63, k = (tid >> 6) + 4 m), m < MG
   double xz[MG];
 #pragma unroll
@@ -141,8 +159,8 @@ __global__ void __launch_bounds__(TPB) grad_hess_kernel(Args a) {
         v0 = fk * fl;
         if (QSIDE) v1 = (1.0 - fk) * (1.0 - fl);
       }
-      s.pp[c * TP + t] = v0;
-      if (QSIDE) s.pp[CJ * TP + c * TP + t] = v1;
+      s.pp[c * PSTR + t] = v0;
+      if (QSIDE) s.pp[CJ * PSTR + c * PSTR + t] = v1;
     }
     // coefficients of the TR x CJ entries; lanes walk the sample axis of G. A thread's
     // entries share one factor row -- its row (tid & 63) on the Q side, its reduced entry
@@ -183,12 +201,12 @@ __global__ void __launch_bounds__(TPB) grad_hess_kernel(Args a) {
         }
       }
       if (QSIDE) {
-        s.coef[c * TR + r] = w1;
-        s.coef[CJ * TR + c * TR + r] = w2;
+        s.coef[c * CSTR + r] = w1;
+        s.coef[CJ * CSTR + c * CSTR + r] = w2;
         s.zc[c * TR + r] = z1;
         s.zc[CJ * TR + c * TR + r] = z2;
       } else {
-        s.coef[c * TR + r] = w1 + w2;
+        s.coef[c * CSTR + r] = w1 + w2;
         s.zc[c * TR + r] = z1 - z2;
       }
     }
@@ -196,19 +214,20 @@ __global__ void __launch_bounds__(TPB) grad_hess_kernel(Args a) {
     const int cmax = (int)min((int64_t)CJ, n_red - red0);
 #pragma unroll
     for (int t = 0; t < NT; ++t) {
-      // the thread's rows are rg + 16 i: the 16 row groups of a warp read 16 consecutive
-      // coefficients (one conflict-free wavefront, the other half-warp a broadcast)
-      const double* cf = s.coef + t * CJ * TR + rg;
-      const double* pr = s.pp + t * CJ * TP + pg * 4;
-      for (int c = 0; c < cmax; ++c) {
-        const double2 b01 = *reinterpret_cast<const double2*>(pr + c * TP);
-        const double2 b23 = *reinterpret_cast<const double2*>(pr + c * TP + 2);
-        const double av[4] = {cf[c * TR], cf[c * TR + 16], cf[c * TR + 32], cf[c * TR + 48]};
-        const double bv[4] = {b01.x, b01.y, b23.x, b23.y};
+      // A (rows x chunk entries) = coef^T, B (chunk entries x pairs) = pp: fragment
+      // element (row fg [+8], entry ft) of A, (entry ft, pair fg) of B
+      const double* cf = s.coef + t * CJ * CSTR + wr * 32 + fg;
+      const double* pr = s.pp + t * CJ * PSTR + wp * 16 + fg;
 #pragma unroll
-        for (int i = 0; i < 4; ++i)
-#pragma unroll
-          for (int j = 0; j < 4; ++j) acc[i][j] = fma(av[i], bv[j], acc[i][j]);
+      for (int c0 = 0; c0 < CJ; c0 += 4) {
+        const double* ca = cf + (c0 + ft) * CSTR;
+        const double* pb = pr + (c0 + ft) * PSTR;
+        const double a00 = ca[0], a01 = ca[8], a10 = ca[16], a11 = ca[24];
+        const double b0 = pb[0], b1 = pb[8];
+        mma_f64(acc[0][0], a00, a01, b0);
+        mma_f64(acc[0][1], a00, a01, b1);
+        mma_f64(acc[1][0], a10, a11, b0);
+        mma_f64(acc[1][1], a10, a11, b1);
       }
     }
     if (do_grad) {
@@ -225,22 +244,25 @@ __global__ void __launch_bounds__(TPB) grad_hess_kernel(Args a) {
     }
   }
 
-  // scatter: both halves of the symmetric Hessian
+  // scatter: both halves of the symmetric Hessian; accumulator v of tile (i, j) is row
+  // fg (+8 for v >= 2), pair 2 ft + (v & 1) of the tile
 #pragma unroll
-  for (int i = 0; i < 4; ++i) {
-    const int64_t row = row0 + rg + 16 * i;
-    if (row >= n_rows) continue;
-    double* H = a.XtX + row * K * K;
+  for (int i = 0; i < 2; ++i)
 #pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      const int t = pg * 4 + j;
-      const int k = s.pk[t];
-      if (k == 0xFF) continue;
-      const int l = s.pl[t];
-      atomicAdd(H + k * K + l, acc[i][j]);
-      if (l != k) atomicAdd(H + l * K + k, acc[i][j]);
+    for (int v = 0; v < 4; ++v) {
+      const int64_t row = row0 + wr * 32 + i * 16 + fg + (v >> 1) * 8;
+      if (row >= n_rows) continue;
+      double* H = a.XtX + row * K * K;
+#pragma unroll
+      for (int j = 0; j < 2; ++j) {
+        const int t = wp * 16 + j * 8 + 2 * ft + (v & 1);
+        const int k = s.pk[t];
+        if (k == 0xFF) continue;
+        const int l = s.pl[t];
+        atomicAdd(H + k * K + l, acc[i][j][v]);
+        if (l != k) atomicAdd(H + l * K + k, acc[i][j][v]);
+      }
     }
-  }
   if (do_grad) {
     const int64_t row = row0 + gr;
     if (row < n_rows) {
