@@ -64,14 +64,14 @@ struct Smem {
   double *own, *fac, *coef, *zc, *pp;
   uint8_t *pk, *pl;
   static __host__ size_t bytes(int K, int nt) {
-    return sizeof(double) * ((size_t)(TR + CJ) * K + (size_t)nt * CJ * (CSTR + TR) + (size_t)nt * CJ * PSTR) + 2 * TP;
+    return sizeof(double) * ((size_t)(TR + CJ) * K + (size_t)nt * CJ * 2 * CSTR + (size_t)nt * CJ * PSTR) + 2 * TP;
   }
   __device__ Smem(uint8_t* base, int K, int nt) {
     double* d = reinterpret_cast<double*>(base);
     own = d; d += TR * K;            // [TR][K] factors of the tile's rows
     fac = d; d += CJ * K;            // [CJ][K] factors of the chunk's reduced entries
     coef = d; d += nt * CJ * CSTR;   // [nt][CJ][CSTR] Hessian coefficients
-    zc = d; d += nt * CJ * TR;       // [nt][CJ][TR] gradient coefficients
+    zc = d; d += nt * CJ * CSTR;     // [nt][CJ][CSTR] gradient coefficients
     pp = d; d += nt * CJ * PSTR;     // [nt][CJ][PSTR] pair products
     pk = reinterpret_cast<uint8_t*>(d);
     pl = pk + TP;
@@ -79,12 +79,12 @@ struct Smem {
 };
 
 // KM: an upper bound of K known at compile time (4, 6, 8, 10, 12, 16, or 64 for the rest),
-// which sizes the gradient's per-thread registers and loops -- thread (row gr,
-// k = gk0 + 4 m) for m < ceil(KM / 4) instead of issuing predicated-off iterations up to
-// K = 64 -- and, for KM <= 16, the factor row kept in registers.
+// which sizes the gradient's MMA tiles (64 rows x ceil(KM / 8) column tiles of 8, spread
+// over the 8 warps) and, for KM <= 16, the factor row kept in registers.
 template <bool QSIDE, int KM>
 __global__ void __launch_bounds__(TPB) grad_hess_kernel(Args a) {
-  constexpr int MG = (KM + 3) / 4;   // gradient entries per thread
+  constexpr int NTG = (KM + 7) / 8;          // gradient column tiles
+  constexpr int GT = (4 * NTG + 7) / 8;      // gradient tiles per warp
   constexpr int NT = QSIDE ? 2 : 1;   // coefficient terms
   extern __shared__ __align__(16) uint8_t smem[];
   const int K = a.K;
@@ -130,11 +130,12 @@ __global__ void __launch_bounds__(TPB) grad_hess_kernel(Args a) {
     for (int j = 0; j < 2; ++j)
 #pragma unroll
       for (int v = 0; v < 4; ++v) acc[i][j][v] = 0.0;
-  // gradient: thread (row r = tid & 63, k = (tid >> 6) + 4 m), m < MG
-  double xz[MG];
+  // gradient: 4 row tiles x NTG column tiles of 16 x 8; warp w owns tiles w, w + 8, ...
+  double gacc[GT][4];
 #pragma unroll
-  for (int m = 0; m < MG; ++m) xz[m] = 0.0;
-  const int gr = tid & (TR - 1), gk0 = tid >> 6;
+  for (int q = 0; q < GT; ++q)
+#pragma unroll
+    for (int v = 0; v < 4; ++v) gacc[q][v] = 0.0;
 
   const int64_t n_chunks = (n_red + CJ - 1) / CJ;
   const int64_t ch0 = (int64_t)split * a.chunks_per_split;
@@ -203,15 +204,14 @@ __global__ void __launch_bounds__(TPB) grad_hess_kernel(Args a) {
       if (QSIDE) {
         s.coef[c * CSTR + r] = w1;
         s.coef[CJ * CSTR + c * CSTR + r] = w2;
-        s.zc[c * TR + r] = z1;
-        s.zc[CJ * TR + c * TR + r] = z2;
+        s.zc[c * CSTR + r] = z1;
+        s.zc[CJ * CSTR + c * CSTR + r] = z2;
       } else {
         s.coef[c * CSTR + r] = w1 + w2;
-        s.zc[c * TR + r] = z1 - z2;
+        s.zc[c * CSTR + r] = z1 - z2;
       }
     }
     __syncthreads();
-    const int cmax = (int)min((int64_t)CJ, n_red - red0);
 #pragma unroll
     for (int t = 0; t < NT; ++t) {
       // A (rows x chunk entries) = coef^T, B (chunk entries x pairs) = pp: fragment
@@ -231,14 +231,21 @@ __global__ void __launch_bounds__(TPB) grad_hess_kernel(Args a) {
       }
     }
     if (do_grad) {
-      for (int c = 0; c < cmax; ++c) {
-        const double* f = s.fac + c * K;
-        const double y1 = s.zc[c * TR + gr];
-        const double y2 = QSIDE ? s.zc[CJ * TR + c * TR + gr] : 0.0;
+      // Xtz += z1' fac (+ z2' (1 - fac) on the Q side): A = z (rows x chunk entries),
+      // B = the chunk's factor rows, columns k >= K fed zeros
 #pragma unroll
-        for (int m = 0; m < MG; ++m) {
-          const int k = gk0 + 4 * m;
-          if (k < K) xz[m] += QSIDE ? (y1 * f[k] + y2 * (1.0 - f[k])) : (y1 * f[k]);
+      for (int q = 0; q < GT; ++q) {
+        const int tix = warp + 8 * q;
+        if (tix >= 4 * NTG) break;   // warp-uniform
+        const int mt = tix & 3, k = (tix >> 2) * 8 + fg;
+        const bool kin = k < K;
+        const double* z = s.zc + mt * 16 + fg;
+#pragma unroll
+        for (int c0 = 0; c0 < CJ; c0 += 4) {
+          const int c = c0 + ft;
+          const double f = kin ? s.fac[c * K + k] : 0.0;
+          mma_f64(gacc[q], z[c * CSTR], z[c * CSTR + 8], f);
+          if (QSIDE) mma_f64(gacc[q], z[(CJ + c) * CSTR], z[(CJ + c) * CSTR + 8], kin ? 1.0 - f : 0.0);
         }
       }
     }
@@ -264,12 +271,16 @@ __global__ void __launch_bounds__(TPB) grad_hess_kernel(Args a) {
       }
     }
   if (do_grad) {
-    const int64_t row = row0 + gr;
-    if (row < n_rows) {
 #pragma unroll
-      for (int m = 0; m < MG; ++m) {
-        const int k = gk0 + 4 * m;
-        if (k < K) atomicAdd(a.Xtz + row * K + k, xz[m]);
+    for (int q = 0; q < GT; ++q) {
+      const int tix = warp + 8 * q;
+      if (tix >= 4 * NTG) break;
+      const int mt = tix & 3, nt = tix >> 2;
+#pragma unroll
+      for (int v = 0; v < 4; ++v) {
+        const int64_t row = row0 + mt * 16 + fg + (v >> 1) * 8;
+        const int k = nt * 8 + 2 * ft + (v & 1);
+        if (row < n_rows && k < K) atomicAdd(a.Xtz + row * K + k, gacc[q][v]);
       }
     }
   }
