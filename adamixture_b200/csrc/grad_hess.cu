@@ -149,19 +149,22 @@ __global__ void __launch_bounds__(TPB) grad_hess_kernel(Args a) {
       s.fac[e] = j < n_red ? redF[j * K + k] : 0.0;
     }
     __syncthreads();
-    // pair products of the chunk's entries (shared by every row)
-    for (int e = tid; e < CJ * TP; e += TPB) {
-      const int c = e / TP, t = e - c * TP;
-      const int k = s.pk[t];
-      double v0 = 0.0, v1 = 0.0;
-      if (k != 0xFF) {
-        const int l = s.pl[t];
-        const double fk = s.fac[c * K + k], fl = s.fac[c * K + l];
-        v0 = fk * fl;
-        if (QSIDE) v1 = (1.0 - fk) * (1.0 - fl);
+    // pair products of the chunk's entries (shared by every row); TPB is a multiple of
+    // TP, so a thread's entries all have pair t = tid % TP
+    {
+      static_assert(TPB % TP == 0, "one pair per thread");
+      const int t = tid & (TP - 1);
+      const int k = s.pk[t], l = s.pl[t];
+      for (int c = tid / TP; c < CJ; c += TPB / TP) {
+        double v0 = 0.0, v1 = 0.0;
+        if (k != 0xFF) {
+          const double fk = s.fac[c * K + k], fl = s.fac[c * K + l];
+          v0 = fk * fl;
+          if (QSIDE) v1 = (1.0 - fk) * (1.0 - fl);
+        }
+        s.pp[c * PSTR + t] = v0;
+        if (QSIDE) s.pp[CJ * PSTR + c * PSTR + t] = v1;
       }
-      s.pp[c * PSTR + t] = v0;
-      if (QSIDE) s.pp[CJ * PSTR + c * PSTR + t] = v1;
     }
     // coefficients of the TR x CJ entries; lanes walk the sample axis of G. A thread's
     // entries share one factor row -- its row (tid & 63) on the Q side, its reduced entry
@@ -184,9 +187,19 @@ __global__ void __launch_bounds__(TPB) grad_hess_kernel(Args a) {
           double h = 0.0;
           if constexpr (KM <= 16) {
             const double* var = QSIDE ? s.fac + c * K : s.own + r * K;
+            if (KM % 2 == 0 && K == KM) {
+              // K even: the row starts 16-byte aligned, read it two doubles at a time
 #pragma unroll
-            for (int k = 0; k < KM; ++k)
-              if (k < K) h += QSIDE ? fix[k] * var[k] : var[k] * fix[k];
+              for (int k = 0; k < KM; k += 2) {
+                const double2 v2 = *reinterpret_cast<const double2*>(var + k);
+                h += QSIDE ? fix[k] * v2.x : v2.x * fix[k];
+                h += QSIDE ? fix[k + 1] * v2.y : v2.y * fix[k + 1];
+              }
+            } else {
+#pragma unroll
+              for (int k = 0; k < KM; ++k)
+                if (k < K) h += QSIDE ? fix[k] * var[k] : var[k] * fix[k];
+            }
           } else {
             for (int k = 0; k < K; ++k) h += s.own[r * K + k] * s.fac[c * K + k];
           }
