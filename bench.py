@@ -558,6 +558,22 @@ def run_kernels(args, cfg):
     fwd_flops = 2.0 * N * (ws.D_IN * ws.H + ws.H * ws.H + ws.H * ws.KMAX)
     timed("mlp_forward", lambda: net.forward(X, prior), None, fwd_flops)
     timed("mlp_forward_backward", lambda: net.gradients(X, prior, T), None, 3 * fwd_flops)
+    # host: the .P text writer (all host threads) against np.savetxt, the same bytes
+    import tempfile
+
+    from adamixture_b200.src import utils as src_utils
+
+    Ph = np.random.default_rng(0).uniform(1e-5, 1 - 1e-5, (M, K))
+    with tempfile.TemporaryDirectory() as d:
+        t0 = time.perf_counter()
+        src_utils.write_outputs(Ph, "native", K, d)
+        t_native = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        np.savetxt(os.path.join(d, "ref.P"), Ph, delimiter=" ")
+        t_np = time.perf_counter() - t0
+        same = Path(d, f"native.{K}.Q").read_bytes() == Path(d, "ref.P").read_bytes()
+    out["write_P_text_host"] = {"ms": t_native * 1e3, "np_savetxt_ms": t_np * 1e3, "identical": same,
+                                "host_threads": os.cpu_count(), "values": M * K}
     line = {"metric": "kernel timings", "config": {"workload": cfg["workload"], "N": N, "M": M, "K": K,
             "note": "CUDA events, mean of 3 launches after one warm-up (Hessian passes: 1); GBps from "
                     "algorithmic bytes, hbm_frac against the measured copy bandwidth"}, "kernels": out}
