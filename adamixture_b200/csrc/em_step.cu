@@ -54,7 +54,7 @@ struct EmPlan {
   size_t ab_elems, t_elems, elem_size;
   // Workspace: a 256-byte header whose first word is the sweep's sticky status (the same
   // offset for every shape, so a shared grow-only buffer keeps it), then the partials.
-  // The tensor-core sweep also keeps a BF16 copy of Q after the partials.
+  // The tensor-core sweep also keeps a 16-bit (FP16 or BF16) copy of Q after the partials.
   static constexpr size_t HEADER = 256;
   size_t extra_bytes = 0;
   size_t extra_offset() const { return (HEADER + (ab_elems + t_elems) * elem_size + 255) & ~size_t(255); }

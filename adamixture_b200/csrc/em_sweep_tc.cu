@@ -51,8 +51,6 @@
 // frees its TMEM and returns.
 #include "common.cuh"
 
-#include <cuda_bf16.h>
-
 #ifndef ADX_TC_HALF_WGS
 #define ADX_TC_HALF_WGS 2
 #endif
