@@ -175,14 +175,26 @@ __global__ void __launch_bounds__(TPB) grad_hess_kernel(Args a) {
 #pragma unroll
       for (int k = 0; k < KM; ++k) fix[k] = k < K ? src[k] : 0.0;
     }
-    for (int e = tid; e < TR * CJ; e += TPB) {
-      int r, c;
-      if (QSIDE) { c = e / TR; r = e - c * TR; } else { r = e / CJ; c = e - r * CJ; }
+    // A thread's 8 entries run along the SNP axis -- Q side: chunk entries 8 (tid >> 6) + n
+    // of row tid & 63; P side: rows 8 (tid >> 5) + n of chunk entry tid & 31 -- so they come
+    // from two packed genotype bytes (SNPs snp0 .. snp0 + 7 of one sample).
+    const int fixed = QSIDE ? (tid & (TR - 1)) : (tid & (CJ - 1));
+    const int first = QSIDE ? 8 * (tid >> 6) : 8 * (tid >> 5);
+    const int64_t smp = (QSIDE ? row0 : red0) + fixed;
+    const int64_t snp0 = (QSIDE ? red0 : row0) + first;   // a multiple of 8
+    uint32_t gbytes = 0xFFFFu;                              // all missing outside the matrix
+    if (smp < a.N) {
+      if (snp0 < a.M) gbytes = (gbytes & 0xFF00u) | (uint32_t)a.G[(snp0 >> 2) * a.N + smp];
+      if (snp0 + 4 < a.M) gbytes = (gbytes & 0x00FFu) | ((uint32_t)a.G[((snp0 >> 2) + 1) * a.N + smp] << 8);
+    }
+#pragma unroll
+    for (int n = 0; n < 8; ++n) {
+      const int r = QSIDE ? fixed : first + n;
+      const int c = QSIDE ? first + n : fixed;
       const int64_t row = row0 + r, red = red0 + c;
       double w1 = 0.0, w2 = 0.0, z1 = 0.0, z2 = 0.0;
       if (row < n_rows && red < n_red) {
-        const int64_t snp = QSIDE ? red : row, smp = QSIDE ? row : red;
-        const unsigned g = genotype(a.G[(snp >> 2) * a.N + smp], (int)(snp & 3));
+        const unsigned g = (gbytes >> (2 * n)) & 3u;   // SNP snp0 + n
         if (g != 3u) {
           double h = 0.0;
           if constexpr (KM <= 16) {
@@ -205,8 +217,14 @@ __global__ void __launch_bounds__(TPB) grad_hess_kernel(Args a) {
           }
           h = fmax(fmin(h, 1.0 - 1e-10), 1e-10);
           const double gd = (double)g, om = 1.0 - h;
-          // one division: 1/h and 1/(1-h) from 1/(h(1-h))
-          const double rr = 1.0 / (h * om);
+          // 1/h and 1/(1-h) from one reciprocal of x = h(1-h) in [1e-10, 0.25]: the hardware
+          // approximation refined by two Newton-Raphson steps r <- r (2 - x r), each of which
+          // squares the relative error (within a unit or two of the last place after both)
+          const double x = h * om;
+          double rr;
+          asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(rr) : "d"(x));
+          rr = fma(rr, fma(-x, rr, 1.0), rr);
+          rr = fma(rr, fma(-x, rr, 1.0), rr);
           const double ih = om * rr, iom = h * rr;
           z1 = gd * ih;
           z2 = (2.0 - gd) * iom;
