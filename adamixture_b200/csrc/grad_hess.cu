@@ -143,10 +143,10 @@ __global__ void __launch_bounds__(TPB) grad_hess_kernel(Args a) {
   for (int64_t ch = ch0; ch < ch1; ++ch) {
     const int64_t red0 = ch * CJ;
     __syncthreads();  // the previous chunk's readers are done
-    for (int e = tid; e < CJ * K; e += TPB) {
-      const int c = e / K, k = e - c * K;
-      const int64_t j = red0 + c;
-      s.fac[e] = j < n_red ? redF[j * K + k] : 0.0;
+    {
+      // the chunk's factor rows are contiguous: a flat copy, zeros past the reduced axis
+      const int64_t base = red0 * K, end = n_red * K;
+      for (int e = tid; e < CJ * K; e += TPB) s.fac[e] = base + e < end ? redF[base + e] : 0.0;
     }
     __syncthreads();
     // pair products of the chunk's entries (shared by every row); TPB is a multiple of
