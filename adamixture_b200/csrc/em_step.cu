@@ -94,6 +94,27 @@ __device__ __forceinline__ R reduce_scatter32(R (&v)[32], int lane) {
   return v[0];
 }
 
+// The same for VR (a power of two below 32) values per lane: the butterfly over the low
+// log2(VR) lane bits leaves lane L with value L & (VR - 1) summed over its group of VR lanes,
+// and a plain xor-sum across the 32 / VR groups completes it: (VR - 1) + log2(32 / VR)
+// shuffles instead of 31 for a vector padded to 32.
+template <int VR, typename R>
+__device__ __forceinline__ R reduce_scatter_small(R (&v)[VR], int lane) {
+#pragma unroll
+  for (int h = VR / 2; h >= 1; h >>= 1) {
+    const bool up = (lane & h) != 0;
+#pragma unroll
+    for (int i = 0; i < h; ++i) {
+      const R send = up ? v[i] : v[i + h];
+      const R keep = up ? v[i + h] : v[i];
+      v[i] = keep + __shfl_xor_sync(0xffffffffu, send, h);
+    }
+  }
+#pragma unroll
+  for (int h = VR; h < 32; h <<= 1) v[0] += __shfl_xor_sync(0xffffffffu, v[0], h);
+  return v[0];
+}
+
 // ---------------------------------------------------------------- E-step sweep
 
 template <typename R, int KMAX>
@@ -169,12 +190,12 @@ em_sweep_kernel(const uint8_t* __restrict__ G, const R* __restrict__ P, const R*
             for (int k = 0; k < KMAX; ++k) tab[u][k] += d * Ps[jl][k];
             tb[u] += b[u];
           }
+          if constexpr (V <= 16) {
+            // at most 16 values: a power-of-two vector of VR, reduced with fewer shuffles
+            constexpr int VR = V <= 4 ? 4 : (V <= 8 ? 8 : 16);
+            R part[VR];
 #pragma unroll
-          for (int c = 0; c < C::NCH; ++c) {
-            R part[32];
-#pragma unroll
-            for (int l = 0; l < 32; ++l) {
-              const int v = c * 32 + l;
+            for (int v = 0; v < VR; ++v) {
               R acc = 0;
               if (v < KMAX) {
 #pragma unroll
@@ -183,9 +204,29 @@ em_sweep_kernel(const uint8_t* __restrict__ G, const R* __restrict__ P, const R*
 #pragma unroll
                 for (int u = 0; u < SPT; ++u) acc += b[u] * q[u][v >= KMAX && v < V ? v - KMAX : 0];
               }
-              part[l] = acc;
+              part[v] = acc;
             }
-            red[warp][jl][c * 32 + lane] = reduce_scatter32(part, lane);
+            // lanes >= VR hold copies of lanes & (VR - 1): slots V.. of red are never read
+            red[warp][jl][lane] = reduce_scatter_small<VR>(part, lane);
+          } else {
+#pragma unroll
+            for (int c = 0; c < C::NCH; ++c) {
+              R part[32];
+#pragma unroll
+              for (int l = 0; l < 32; ++l) {
+                const int v = c * 32 + l;
+                R acc = 0;
+                if (v < KMAX) {
+#pragma unroll
+                  for (int u = 0; u < SPT; ++u) acc += a[u] * q[u][v < KMAX ? v : 0];
+                } else if (v < V) {
+#pragma unroll
+                  for (int u = 0; u < SPT; ++u) acc += b[u] * q[u][v >= KMAX && v < V ? v - KMAX : 0];
+                }
+                part[l] = acc;
+              }
+              red[warp][jl][c * 32 + lane] = reduce_scatter32(part, lane);
+            }
           }
         }
       }
