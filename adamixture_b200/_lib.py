@@ -60,6 +60,7 @@ SIGNATURES: dict[str, list] = {
     "adx_cv_deviance_list": [P, I64, I64, c_int, P, P, P, I64, P, P, c_size_t, P],
     "adx_cv_deviance_hash": [P, I64, I64, c_int, P, P, c_uint64, c_int, c_int, P, P, c_size_t, P],
     "adx_write_text_matrix": [ctypes.c_char_p, P, I64, I64, c_int],
+    "adx_tc_wait_selftest": [c_int, c_uint32, P, P],
     "adx_write_text_matrix_fixed": [ctypes.c_char_p, P, I64, I64, c_int, c_int],
     "adx_mlp_workspace_bytes": [I64, c_int, P],
     "adx_mlp_forward": [P, P, P, P, P, P, P, P, I64, c_int, P, P, c_size_t, P],

@@ -156,9 +156,11 @@ __device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
   return ok != 0;
 }
 
-// Bounded wait; returns false on timeout or when another warp has aborted.
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatile int* abort_flag) {
-  for (uint32_t it = 0; it < WAIT_LIMIT; ++it) {
+// Bounded wait; returns false on timeout (raising the abort word) or when another warp has
+// aborted.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatile int* abort_flag,
+                                          uint32_t limit = WAIT_LIMIT) {
+  for (uint32_t it = 0; it < limit; ++it) {
     if (mbar_try(bar, parity)) return true;
     if (*abort_flag) return false;
     if (it > 64) __nanosleep(32);
@@ -639,6 +641,31 @@ __global__ void __launch_bounds__(TPB, 1) em_sweep_tc_kernel(Args a) {
   }
 }
 
+// Self-test of the bounded wait above: one mbarrier expecting one arrival. With arrive = 0
+// nothing arrives, so thread 0's wait gives up after `limit` polls, reports ADX_ERR_TIMEOUT
+// and raises the abort word, and a second warp's wait on the same barrier must then leave
+// at once; with arrive = 1 both waits complete. status[0..2]: the first wait's result, the
+// abort word, the second wait's result.
+__global__ void wait_selftest_kernel(int arrive, uint32_t limit, int* status) {
+  __shared__ __align__(8) uint64_t bar_word;
+  __shared__ int abort_word;
+  const uint32_t bar = smem_u32(&bar_word);
+  if (threadIdx.x == 0) {
+    abort_word = 0;
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar));
+    asm volatile("fence.mbarrier_init.release.cluster;");
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    if (arrive) mbar_arrive(bar);
+    const bool ok = mbar_wait(bar, 0u, &abort_word, limit);
+    status[0] = ok ? ADX_OK : ADX_ERR_TIMEOUT;
+    status[1] = abort_word;
+  }
+  __syncthreads();
+  if (threadIdx.x == 32) status[2] = mbar_wait(bar, 0u, &abort_word, limit) ? ADX_OK : ADX_ERR_TIMEOUT;
+}
+
 }  // namespace tc
 
 int tc_plan(int64_t M, int64_t N, int K, int64_t& n_stile, int& n_split, int& n_mblk) {
@@ -668,6 +695,16 @@ static int tc_launch(const tc::Args& a, int64_t n_stile, uint8_t* qb, const floa
                                                                                                 n_stile, qb);
   ADX_LAUNCH_CHECK();
   tc::em_sweep_tc_kernel<F16><<<(unsigned)(a.n_split * a.n_mblk), tc::TPB, tc::SMEM_ALLOC, st>>>(a);
+  ADX_LAUNCH_CHECK();
+  return ADX_OK;
+}
+
+extern "C" int adx_tc_wait_selftest(int arrive, uint32_t limit, int* status, void* stream) {
+  if (!status || limit < 1) {
+    adx_set_message("adx_tc_wait_selftest: bad argument");
+    return ADX_ERR_ARG;
+  }
+  tc::wait_selftest_kernel<<<1, 64, 0, as_stream(stream)>>>(arrive, limit, status);
   ADX_LAUNCH_CHECK();
   return ADX_OK;
 }

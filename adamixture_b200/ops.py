@@ -185,6 +185,15 @@ def em_status(workspace: torch.Tensor, M: int, N: int, K: int, precision) -> int
     return int(out.value)
 
 
+def tc_wait_selftest(arrive: bool, limit: int, device=None) -> list[int]:
+    """Run the tensor-core sweep's bounded-wait self-test on ``device``: ``[first wait's
+    status, abort word, second wait's status]`` (ADX_OK = 0, ADX_ERR_TIMEOUT = 5)."""
+    dev = torch.device("cuda", torch.cuda.current_device()) if device is None else torch.device(device)
+    status = torch.full((3,), -1, dtype=torch.int32, device=dev)
+    call("adx_tc_wait_selftest", int(bool(arrive)), int(limit), status.data_ptr(), _stream(dev))
+    return [int(v) for v in status.cpu().tolist()]
+
+
 def em_sweep(G: torch.Tensor, P: torch.Tensor, Q: torch.Tensor, M: int, precision,
              workspace: torch.Tensor) -> None:
     """The E-step sweep alone (partials left in ``workspace``)."""

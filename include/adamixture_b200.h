@@ -99,6 +99,13 @@ int adx_em_workspace_bytes(int64_t M, int64_t N, int K, int precision, size_t* b
  * bounded wait for its tensor-core work gave up). Synchronises `stream`. */
 int adx_em_status(void* workspace, size_t workspace_bytes, int64_t M, int64_t N, int K,
                   int precision, int* status, void* stream);
+/* Self-test of the bounded mbarrier wait the tensor-core sweep uses for every producer /
+ * consumer hand-off (no counterpart in the reference): one barrier expecting one arrival;
+ * arrive = 0 leaves it unarrived, so the wait must give up after `limit` polls. Writes three
+ * ints to the device array `status`: the first wait's result (ADX_OK or ADX_ERR_TIMEOUT),
+ * the abort word a timed-out wait raises (0/1), and a second warp's wait on the same barrier
+ * (which must leave at once once the abort word is up). No GPU fault or hang either way. */
+int adx_tc_wait_selftest(int arrive, uint32_t limit, int* status, void* stream);
 
 /* One fused E-step sweep over G: A, B [M][K] and T [N][K] (float64), the sufficient
  * statistics EMAdamOptimizer.run_em_step accumulates (A_accum, B_accum, T_accum;

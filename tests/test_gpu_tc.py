@@ -106,6 +106,29 @@ def test_tc_status_word_clear(ops, prec, synth):
     assert ops.em_status(ws, M, N, K, prec) == 0
 
 
+def test_bounded_wait_gives_up_and_reports(ops):
+    # the wait the sweep uses at every producer/consumer hand-off, on a barrier nothing
+    # arrives at: it gives up after its poll limit, reports a timeout and raises the abort
+    # word, which a second waiting warp honours at once; with the arrival both complete
+    assert ops.tc_wait_selftest(False, 2000) == [5, 1, 5]
+    assert ops.tc_wait_selftest(True, 2000) == [0, 0, 0]
+
+
+def test_optimiser_raises_on_a_sweep_timeout(ops, synth):
+    # a sweep that timed out leaves ADX_ERR_TIMEOUT in its workspace's status word; the
+    # optimiser's next check must raise (here the word is set by hand), and the read clears it
+    from adamixture_b200.model.em_adam_gpu import optimize_parameters_gpu
+
+    M, N, K = int(synth["M"]), int(synth["N"]), int(synth["K"])
+    G = dev_t(synth["packed"])
+    ws = ops.Workspace.get(G.device, ops.em_workspace_bytes(M, N, K, "f16"))
+    ws[:4].copy_(torch.tensor([5, 0, 0, 0], dtype=torch.uint8))
+    with pytest.raises(RuntimeError, match="status 5"):
+        optimize_parameters_gpu(G, dev_t(synth["P0"]), dev_t(synth["Q0"]), 0.005, 0.80, 0.88, 1e-8, 10, 5, K,
+                                M, N, 0.5, 1e-4, 3, 0.1, G.device, 8192, 512, precision="f16")
+    assert ops.em_status(ws, M, N, K, "f16") == 0
+
+
 @pytest.mark.parametrize("name", ["demo", "synth"])
 def test_tc_converged_loglik(ops, prec, name, request):
     from adamixture_b200.model.em_adam_gpu import loglikelihood_gpu, optimize_parameters_gpu
