@@ -120,6 +120,30 @@ def test_projection_adamem_matches_reference(cuda, cv_proj):
     np.testing.assert_allclose(Q.cpu().numpy(), cv_proj["proj_adamem_Q"], atol=1e-5)
 
 
+@pytest.mark.parametrize("prec,bar", [("f16", 1e-6), ("bf16", 1e-5), ("f32", 1e-6)])
+def test_projection_in_reduced_precision(cuda, synth, prec, bar):
+    # K = 8: the tensor-core forms (the default FP16 one among them) and float32 project to
+    # the float64 projection's fit: log-likelihood within `bar` relative (BF16's operands
+    # stop it further away). Both runs stop once a check gains less than tol = 0.1, so Q
+    # may differ along flat directions (observed for FP16: 3.5 % of entries by up to 5e-3
+    # at a 1.2e-9 higher log-likelihood): Q is held to a mean difference of 1e-3.
+    from adamixture_b200.model.em_adam_gpu import loglikelihood_gpu
+    from adamixture_b200.src.projection import optimize_projection_gpu
+
+    M, N = int(synth["M"]), int(synth["N"])
+    G = dev(synth["packed"])
+    P = dev(synth["conv_P"])
+    out = {}
+    for p in ("f64", prec):
+        Q = optimize_projection_gpu(G, P, dev(synth["Q0"]), 0.005, 0.80, 0.88, 1e-8, 10000, 5, M, 0.5, 1e-4, 3,
+                                    0.1, G.device, 8192, 256, precision=p)
+        out[p] = (Q.cpu().numpy(), loglikelihood_gpu(G, P, Q, M, N, 8192, G.device, 256))
+    dQ = np.abs(out[prec][0] - out["f64"][0])
+    print(prec, "projection loglik", out[prec][1], "float64", out["f64"][1], "max |dQ|", dQ.max(), "mean", dQ.mean())
+    assert abs(out[prec][1] - out["f64"][1]) <= bar * abs(out["f64"][1])
+    assert dQ.mean() <= 1e-3 and dQ.max() <= 5e-2
+
+
 def test_projection_brqn_matches_reference(cuda, cv_proj):
     from adamixture_b200.src.projection import optimize_projection_original_gpu
 
