@@ -20,7 +20,9 @@ namespace adx {
 namespace cv {
 
 constexpr int TPB = 256;
-constexpr int BLOCKS = 1184;   // partials of a deviance sum (8 per SM on 148 SMs)
+// partials of a deviance sum: 40 per SM on 148 SMs, whole waves at 4, 5 (the deviance
+// kernels hold 5) or 8 resident blocks per SM
+constexpr int BLOCKS = 5920;
 
 __device__ __forceinline__ uint64_t fold_hash(uint64_t flat, uint64_t seed) {
   uint64_t h = flat + seed + 0x9E3779B97F4A7C15ull;

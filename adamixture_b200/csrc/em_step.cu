@@ -27,8 +27,10 @@ namespace adx {
 
 constexpr int TPB = 256;
 constexpr int WARPS = TPB / 32;
-constexpr int PLAN_BLOCKS = 592;  // target block count (4 per SM on 148 SMs); fixed so the
-                                  // partition, hence the summation order, never depends on the GPU
+// Block count of a sweep, at most (12 per SM on 148 SMs: whole waves at 1, 2, 3, 4 or 6
+// resident blocks per SM, which covers every instance); fixed so the partition, hence the
+// summation order, never depends on the GPU.
+constexpr int PLAN_BLOCKS = 1776;
 
 template <typename R, int KMAX>
 struct EmCfg {
@@ -429,7 +431,7 @@ int em_plan(int64_t M, int64_t N, int K, int prec, EmPlan& pl) {
   n_split = n_split < 1 ? 1 : n_split;
   n_split = n_split > pl.n_stile ? pl.n_stile : n_split;
   int64_t max_mblk = ceil_div(M, CH);
-  int64_t n_mblk = ceil_div(PLAN_BLOCKS, n_split);
+  int64_t n_mblk = PLAN_BLOCKS / n_split;  // the grid stays within PLAN_BLOCKS
   n_mblk = n_mblk < 1 ? 1 : (n_mblk > max_mblk ? max_mblk : n_mblk);
   int64_t mb = ceil_div(ceil_div(M, n_mblk), CH) * CH;
   n_mblk = ceil_div(M, mb);

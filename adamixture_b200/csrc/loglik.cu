@@ -10,6 +10,12 @@
 // float64 rounding (each multiply adds <= 2^-53 relative error, i.e. <= 1.1e-16 absolute in
 // the log). h is formed in float64 (ADX_F64) or float32 (ADX_F32) from P and Q of that type;
 // with a float32 h the factor is formed in float32 too (the running product stays float64).
+// The float32 path holds P scaled by 2^31 (exact: a power of two), so h, 1-h and f come out
+// scaled by 2^31, 2^31 and 2^62 with the same roundings; a factor then lies in
+// [2^62 1e-20, 2^62] = [0.046, 4.6e18] and the product of two of them in [2.1e-3, 2.1e37], a
+// normal float32. The two factors of an entry pair are multiplied in float32 (one more
+// rounding, 2^-24 relative) and the pair goes into the float64 product with one conversion
+// and one multiply; the 2^248 of every packed quad is taken off the exponent at the end.
 // Per-block float64 partials are summed by a one-block kernel in block order: deterministic.
 #include "common.cuh"
 
@@ -21,7 +27,11 @@
 namespace adx {
 
 constexpr int LL_TPB = 256;
-constexpr int LL_BLOCKS = 1184;  // 8 per SM on 148 SMs; fixed, so the summation order does not depend on the GPU
+// 12 per SM on 148 SMs: whole waves at 1, 2, 3, 4 or 6 resident blocks per SM (the instances
+// hold 1 to 4); fixed, so the summation order does not depend on the GPU
+constexpr int LL_BLOCKS = 1776;
+constexpr float LL_SCALE = 2147483648.0f;  // 2^31: float32 P is held x LL_SCALE
+constexpr int LL_QUAD_EXP = 248;          // a quad's four factors carry (2^62)^4
 
 template <typename R, int KMAX>
 struct LlCfg {
@@ -98,6 +108,7 @@ loglik_kernel(const uint8_t* __restrict__ G, const R* __restrict__ P, const R* _
     unsigned long long qp[PAIRS ? SPT / 2 : 1][KMAX];         // packed path: {q_u, q_u+1}
     double prod[SPT];
     int ex[SPT];
+    int quads = 0;  // packed quads folded into prod (float32 path: 2^248 each to take off)
     auto qval = [&](int u, int k) -> R { return (i0 + u < N && k < K) ? Q[(i0 + u) * K + k] : (R)0; };
 #pragma unroll
     for (int u = 0; u < SPT; ++u) {
@@ -120,7 +131,8 @@ loglik_kernel(const uint8_t* __restrict__ G, const R* __restrict__ P, const R* _
       __syncthreads();
       for (int e = threadIdx.x; e < CH * KMAX; e += LL_TPB) {
         const int jl = e / KMAX, k = e % KMAX;
-        const R v = (jl < cn && k < K) ? P[(c0 + jl) * K + k] : (R)0;
+        R v = (jl < cn && k < K) ? P[(c0 + jl) * K + k] : (R)0;
+        if constexpr (sizeof(R) == 4) v *= LL_SCALE;
         if constexpr (PAIRS) Ps2[jl][k] = pack_f32x2((float)v, (float)v);
         else Ps[jl][k] = v;
       }
@@ -132,6 +144,7 @@ loglik_kernel(const uint8_t* __restrict__ G, const R* __restrict__ P, const R* _
         // no early exit for a ragged chunk end (only the last chunk, when M % 4 != 0): the
         // entries past it count as missing (factor 1), so the four SNPs' dot products are
         // independent and interleave (Ps rows past cn are zeros, inside the CH-row tile)
+        float fpair[SPT];  // float32 path: the scaled factor of the pair's first entry
 #pragma unroll
         for (int s = 0; s < 4; ++s) {
           const int jl = qd + s;
@@ -162,11 +175,12 @@ loglik_kernel(const uint8_t* __restrict__ G, const R* __restrict__ P, const R* _
             if constexpr (sizeof(R) == 4) {
               // float32 h: the factor in float32 as well (its rounding, 6e-8 relative, is below
               // that of h itself); the clamp h in [1e-10, 1-1e-10] is applied to h and to 1-h,
-              // since 1-1e-10 is not a float32 value; f >= 1e-20 stays a normal float
-              const float hf = fmaxf(h[u], (float)LL_CLAMP);
-              const float om = fmaxf(1.0f - h[u], (float)LL_CLAMP);
-              const float f = g == 0u ? om * om : (g == 1u ? hf * om : (g == 2u ? hf * hf : 1.0f));
-              prod[u] *= (double)f;
+              // since 1-1e-10 is not a float32 value. All three are x2^31 (h, 1-h) and x2^62 (f).
+              const float hf = fmaxf(h[u], (float)LL_CLAMP * LL_SCALE);
+              const float om = fmaxf(LL_SCALE - h[u], (float)LL_CLAMP * LL_SCALE);
+              const float f = g == 0u ? om * om : (g == 1u ? hf * om : (g == 2u ? hf * hf : LL_SCALE * LL_SCALE));
+              if (s & 1) prod[u] *= (double)(fpair[u] * f);
+              else fpair[u] = f;
             } else {
               const double hd = fmin(fmax((double)h[u], LL_CLAMP), 1.0 - LL_CLAMP);
               const double om = 1.0 - hd;
@@ -177,10 +191,12 @@ loglik_kernel(const uint8_t* __restrict__ G, const R* __restrict__ P, const R* _
         }
 #pragma unroll
         for (int u = 0; u < SPT; ++u) prod[u] = renorm(prod[u], ex[u]);
+        ++quads;
       }
     }
+    const double off = sizeof(R) == 4 ? (double)LL_QUAD_EXP * (double)quads : 0.0;
 #pragma unroll
-    for (int u = 0; u < SPT; ++u) acc += log(prod[u]) + (double)ex[u] * 0.69314718055994530942;
+    for (int u = 0; u < SPT; ++u) acc += log(prod[u]) + ((double)ex[u] - off) * 0.69314718055994530942;
   }
   // block reduction in fixed order
 #pragma unroll
@@ -247,7 +263,9 @@ static int ll_plan(int64_t M, int64_t N, int K, int prec, LlPlan& pl) {
   pl.spt = spt;
   pl.n_stile = ceil_div(N, (int64_t)LL_TPB * spt);
   int64_t n_split = pl.n_stile < 8 ? pl.n_stile : 8;
-  int64_t n_mblk = ceil_div(LL_BLOCKS, n_split);
+  // at most LL_BLOCKS blocks (rounding the SNP blocks up to 32 rows only lowers the count),
+  // so the grid never spills a few blocks into one more wave
+  int64_t n_mblk = LL_BLOCKS / n_split;
   const int64_t max_mblk = ceil_div(M, 32);
   n_mblk = n_mblk > max_mblk ? max_mblk : n_mblk;
   int64_t mb = ceil_div(ceil_div(M, n_mblk), 32) * 32;
@@ -303,9 +321,8 @@ extern "C" int adx_loglik(const uint8_t* G, int64_t M, int64_t N, int K, int pre
 // partial sums; this variant keeps them in a file-scope device array instead.
 //
 // Limit: the array holds ADX_LL_NOALLOC_MAX_PARTIALS float64 partial sums (16 KiB) on every
-// GPU that loads the library, until the process exits. The launch plan uses fewer than
-// 1200 partials for any M, N and K (LL_BLOCKS rounded up to a multiple of the split
-// count), so every problem size fits; a plan that needed more would be rejected with
+// GPU that loads the library, until the process exits. The launch plan uses at most
+// LL_BLOCKS = 1776 partials for any M, N and K, so every problem size fits; a plan that needed more would be rejected with
 // ADX_ERR_WORKSPACE.
 //
 // Set-up: host code cannot use the array's name as a device address (it names a host-side

@@ -156,7 +156,7 @@ int adx_loglik(const uint8_t* G, int64_t M, int64_t N, int K, int precision, con
  * whose device memory belongs to another allocator, or a code path that cannot accept the
  * device-wide synchronisation of cudaMalloc/cudaFree). No counterpart in the reference.
  * The per-block partial sums live in a 16 KiB file-scope device array instead of a
- * workspace; every problem size fits (the plan never needs 1200 partials; the array holds
+ * workspace; every problem size fits (the plan never needs more than 1776 partials; the array holds
  * 2048, and a larger plan would be rejected with ADX_ERR_WORKSPACE).
  * The first call on a device (with it current) looks up the array's address; make it
  * before any stream capture. Calls share the array: calls that overlap on the GPU race.
