@@ -176,16 +176,22 @@ loglik_kernel(const uint8_t* __restrict__ G, const R* __restrict__ P, const R* _
               // float32 h: the factor in float32 as well (its rounding, 6e-8 relative, is below
               // that of h itself); the clamp h in [1e-10, 1-1e-10] is applied to h and to 1-h,
               // since 1-1e-10 is not a float32 value. All three are x2^31 (h, 1-h) and x2^62 (f).
+              // f = x * y from the genotype's two bits: g=0 om*om, g=1 om*hf, g=2 hf*hf, missing
+              // 2^31*2^31 (the scaled 1), the same products as a four-way select, with two
+              // selects and one multiply
               const float hf = fmaxf(h[u], (float)LL_CLAMP * LL_SCALE);
               const float om = fmaxf(LL_SCALE - h[u], (float)LL_CLAMP * LL_SCALE);
-              const float f = g == 0u ? om * om : (g == 1u ? hf * om : (g == 2u ? hf * hf : LL_SCALE * LL_SCALE));
+              const bool miss = g == 3u, gz = g == 0u;
+              const float hf3 = miss ? LL_SCALE : hf;
+              const float f = ((g & 2u) ? hf3 : om) * (gz ? om : hf3);
               if (s & 1) prod[u] *= (double)(fpair[u] * f);
               else fpair[u] = f;
             } else {
               const double hd = fmin(fmax((double)h[u], LL_CLAMP), 1.0 - LL_CLAMP);
               const double om = 1.0 - hd;
-              const double f = g == 0u ? om * om : (g == 1u ? hd * om : (g == 2u ? hd * hd : 1.0));
-              prod[u] *= f;
+              const bool miss = g == 3u, gz = g == 0u;
+              const double hd3 = miss ? 1.0 : hd;
+              prod[u] *= ((g & 2u) ? hd3 : om) * (gz ? om : hd3);  // the float32 form's two selects
             }
           }
         }
