@@ -48,7 +48,7 @@ def check_run_options(p: argparse.ArgumentParser, a: argparse.Namespace) -> None
     """The reference's parameter checks of these commands (adamixture/project_entry.py:141-158),
     as argument errors."""
     if a.device not in ("cuda", "gpu"):
-        p.error("this build runs on the GPU only (--device cuda)")
+        p.error("adamixture_b200 runs on the GPU only (--device cuda)")
     checks = ((a.threads >= 1, "--threads must be at least 1"), (a.lr > 0, "--lr must be positive"),
               (0 <= a.beta1 < 1, "--beta1 must be in [0, 1)"), (0 <= a.beta2 < 1, "--beta2 must be in [0, 1)"),
               (0 < a.lr_decay <= 1, "--lr_decay must be in (0, 1]"), (a.min_lr > 0, "--min_lr must be positive"),
@@ -110,7 +110,7 @@ def parse_args(argv: list[str]) -> argparse.Namespace:
     p.add_argument("--precision", choices=["f64", "f32", "bf16", "f16", "mixed", "auto"], default=None)
     a = p.parse_args(argv)
     if a.device != "gpu":
-        p.error("this build runs on the GPU only (--device gpu)")
+        p.error("adamixture_b200 runs on the GPU only (--device gpu)")
     if (a.k is None) == (a.min_k is None or a.max_k is None):
         p.error("give either -k or both --min_k and --max_k")
     ks = [a.k] if a.k is not None else list(range(a.min_k, a.max_k + 1))

@@ -8,7 +8,7 @@ Reads P (whitespace-delimited text, M rows x K columns), clamps it to [1e-5, 1 -
 starts Q from ``default_rng(seed).random((N, K))`` with rows normalised, runs the Adam-EM
 projection or the SQP + ZAL quasi-Newton projection on the GPU and writes
 ``{name}.{K}.Q`` with "%.6f" values, as the reference does (project_entry.py:203-291).
-Plots are not produced by this build; ``--plot`` is accepted and ignored with a warning.
+Plots are not produced by this package; ``--plot`` is accepted and ignored with a warning.
 """
 from __future__ import annotations
 
@@ -49,7 +49,7 @@ def run(args: argparse.Namespace, t0: float) -> int:
     from .src.projection import optimize_projection_gpu, optimize_projection_original_gpu
 
     if args.plot is not None:
-        log.warning("    Plotting is not available in this build; --plot is ignored.")
+        log.warning("    Plotting is not available in this package; --plot is ignored.")
     p_path = Path(args.p_path)
     if not p_path.exists():
         log.error(f"    Error: P matrix file not found: {p_path}")

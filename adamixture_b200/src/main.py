@@ -4,7 +4,7 @@ Reads the data once (decoded on the GPU), runs the one-time setup at K_max, trai
 requested K (single K or a min..max sweep, one or several initialisations), aligns each
 K's clusters to the previous K's, writes ``{name}.{K}.Q`` / ``.P`` in the reference's text
 format and, with ``--cv``, scores every K by cross-validation on the GPU afterwards.
-Plots are not produced by this build (no plotting stack); the plot options are accepted
+Plots are not produced by this package (no plotting stack); the plot options are accepted
 and ignored with a warning.
 """
 from __future__ import annotations
@@ -32,7 +32,7 @@ def main(args: argparse.Namespace, t0: float) -> int:
         else:
             k_values = [int(args.k)]
         if getattr(args, "plot", None) is not None or getattr(args, "plot_single", None) is not None:
-            log.warning("    Plotting is not available in this build; --plot options are ignored.")
+            log.warning("    Plotting is not available in this package; --plot options are ignored.")
         n_inits = int(args.n_inits)
         K_max = max(k_values)
         Path(args.save_dir).mkdir(parents=True, exist_ok=True)

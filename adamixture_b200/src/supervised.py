@@ -9,7 +9,7 @@ after each Q solve and after the extrapolated point (supervised.py:602-760).
 
 Parity note: the reference's Adam-EM loop decays a local copy of the learning rate that
 its optimiser never reads (supervised.py:441-451): the Adam step keeps the initial rate and
-the decayed copy only drives the stop. This build does the same, so it returns the same
+the decayed copy only drives the stop. This package does the same, so it returns the same
 model.
 """
 from __future__ import annotations

@@ -21,7 +21,7 @@ def read_data(data_path: str, packed: bool = True, chunk_size: int = 8192, chrom
     ``packed`` is False (adamixture/src/utils.py:read_data, BED branch)."""
     path = Path(data_path)
     if path.suffix not in (".bed", ""):
-        raise ValueError(f"{data_path}: only PLINK .bed input is supported by this build")
+        raise ValueError(f"{data_path}: only PLINK .bed input is supported by this package")
     G, N, M = read_bed_packed(path, chrom_mode, autosomes, specific_chrom, device=device)
     if verbose:
         log.info(f"    Data loaded: {N} samples, {M} SNPs.")

@@ -12,7 +12,7 @@ is the number of distinct names (supervised_entry.py:149-190, 294-304). P starts
 labelled samples' allele frequencies, Q from ``default_rng(seed).random((N, K))`` with the
 labelled rows set near one-hot (supervised_entry.py:309-315); the outputs are
 ``{name}.{K}.Q`` and ``{name}.{K}.P`` with "%.6f" values (supervised_entry.py:380-391).
-Plots are not produced by this build; ``--plot`` is accepted and ignored with a warning.
+Plots are not produced by this package; ``--plot`` is accepted and ignored with a warning.
 """
 from __future__ import annotations
 
@@ -83,7 +83,7 @@ def run(args: argparse.Namespace, t0: float) -> int:
                                  optimize_supervised_original_gpu)
 
     if args.plot is not None:
-        log.warning("    Plotting is not available in this build; --plot is ignored.")
+        log.warning("    Plotting is not available in this package; --plot is ignored.")
     sup_path = Path(getattr(args, {1: "labels", 2: "labels2", 3: "labels3"}[args.level]))
     if not sup_path.exists():
         log.error(f"    Error: Labels file not found: {sup_path}")

@@ -245,7 +245,7 @@ int adx_write_text_matrix_fixed(const char* path, const double* X, int64_t rows,
                                 int decimals, int threads);
 
 /* ---------------------------------------------------------------- warm-start network
- * No counterpart in the reference (a new component of this build). A per-sample network
+ * No counterpart in the reference (a new component of this library). A per-sample network
  * 33 -> 256 -> 256 -> K (K <= 16), GELU hidden layers, output softmax(f(x) + prior) with
  * prior [B][K] optional (log of the ALS memberships, so an untrained network reproduces the
  * ALS start). Weights BF16 (uint16 bit patterns) [out][in], biases and activations float32.

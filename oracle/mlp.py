@@ -2,7 +2,7 @@
 and backward passes (33 -> 256 -> 256 -> K, exact-erf GELU, softmax(f(x) + prior),
 mean cross-entropy against soft targets), used to check the CUDA kernels' outputs and
 gradients. The weights given are the BF16-rounded values the kernels read. (The network
-is this build's own component; the reference has none.)"""
+is this library's own component; the reference has none.)"""
 from __future__ import annotations
 
 import math
