@@ -334,7 +334,9 @@ extern "C" int adx_loglik(const uint8_t* G, int64_t M, int64_t N, int K, int pre
 // Set-up: host code cannot use the array's name as a device address (it names a host-side
 // stand-in). The first call on each device, with that device current, looks the address
 // up with cudaGetSymbolAddress and caches it; make that first call before any stream
-// capture begins. The array is shared by every call and keeps the previous call's
+// capture begins. The cached address belongs to the device's current primary context: a
+// process that calls cudaDeviceReset (which can reload the module at another address)
+// must not call this entry point on that device afterwards. The array is shared by every call and keeps the previous call's
 // contents; each call overwrites every partial it reads, so nothing needs clearing. Two
 // calls whose launches overlap on the GPU (different streams, no ordering) race on it.
 

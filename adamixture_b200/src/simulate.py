@@ -79,7 +79,9 @@ def sample_genotypes(Pq: np.ndarray, Qq: np.ndarray, miss_q: int, keys: tuple[in
     N = Qq.shape[0]
     if m_count is None:
         m_count = M - m_start
-    hq = Pq[m_start:m_start + m_count].astype(np.uint64) @ Qq.T.astype(np.uint64)
+    # every product and partial sum of h_q is an integer <= 2^32, so a float64 product
+    # (BLAS) is exact in any summation order
+    hq = (Pq[m_start:m_start + m_count].astype(np.float64) @ Qq.T.astype(np.float64)).astype(np.uint64)
     j = np.arange(m_start, m_start + m_count, dtype=np.uint64)[:, None]
     i = np.arange(N, dtype=np.uint64)[None, :]
     k1, k2 = (np.uint64(k) for k in keys)
@@ -111,6 +113,23 @@ class Cohort:
 
     def genotypes(self, m_start: int = 0, m_count: int | None = None) -> np.ndarray:
         return sample_genotypes(self.Pq, self.Qq, self.miss_q, self.keys, m_start, m_count)
+
+    def genotypes_parallel(self, m_start: int, m_count: int, threads: int | None = None,
+                           rows_per_task: int = 64) -> np.ndarray:
+        """The same rows as ``genotypes``, sampled by several host threads (numpy releases
+        the interpreter lock inside its array operations) into one ``[m_count, N]`` array."""
+        import os
+        from concurrent.futures import ThreadPoolExecutor
+
+        out = np.empty((m_count, self.N), dtype=np.uint8)
+
+        def task(s):
+            n = min(rows_per_task, m_count - s)
+            out[s:s + n] = self.genotypes(m_start + s, n)
+
+        with ThreadPoolExecutor(threads or os.cpu_count() or 1) as ex:
+            list(ex.map(task, range(0, m_count, rows_per_task)))
+        return out
 
     def packed(self, block: int = 65536) -> np.ndarray:
         """Packed ``[ceil(M/4), N]`` genotypes, built on the host in SNP blocks."""

@@ -2,7 +2,7 @@
 """Benchmark of the ADMIXTURE Adam-EM hot path on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--precision auto|f32|f64|bf16|f16] [--config c3|c2|c1]
+                    [--precision f64|f32|bf16|f16] [--config c3|c2|c1|c3s]
 
 Workload (default ``c3``): N=200,000 samples, M=500,000 SNPs, K=10; a seeded synthetic
 admixed cohort (Balding-Nichols F=0.02; Q 70% Dirichlet(0.05) / 30% Dirichlet(1); 1%
@@ -14,14 +14,22 @@ reference's ``.item()`` does). P/Q start from the reference's random EM initiali
 (adamixture/src/adamixture.py:140-156). Inputs (25 GB) exceed L2 (126 MB), so no flush is
 needed between steps.
 
-One JSON line on rank 0. ``value`` = EM iterations/s (device-timed, max over ranks);
-``e2e`` = the same iterations through the public Python API starting from pinned host
-buffers (packed G, P, Q) and ending with P/Q back on the host; ``roofline`` = the E-step
-sweep kernel alone (algorithmic bytes: ceil(M/4)*N + 4K(3M+2N) per launch) against the
-measured HBM copy bandwidth; ``cpu_baseline`` = the reference's own CPU Adam-EM step
-(its Cython kernels compiled from source into oracle/_ref) on a SNP-row slice of the same
-cohort, scaled linearly to the full M.
-``--impl reference`` prints the reference arm: that CPU implementation as the headline.
+One JSON line on rank 0. The headline ``value`` (EM iterations/s, device-timed, max over
+ranks) is float64 arithmetic throughout, the reference GPU path's own arithmetic
+(``--precision`` changes it). ``variants`` repeats the measurement for the float32 sweep
+and the two tensor-core sweeps (FP16 / BF16 operands, FP32 accumulation), each with its
+own roofline, from the same start. ``time_to_target`` times whole fits from the
+reference's default start (randomized SVD + ALS) to the first check within 1e-6 relative
+of the plain float32 fit's log-likelihood: float32, FP16, and the learned warm start in
+front of FP16. ``e2e`` = the headline iterations through the public Python API starting
+from pinned host buffers (packed G, P, Q) and ending with P/Q back on the host;
+``roofline`` = the headline's E-step sweep kernel alone (algorithmic bytes:
+ceil(M/4)*N + 4K(3M+2N) per launch) against the measured HBM copy bandwidth;
+``cpu_baseline`` = the reference's own CPU Adam-EM step (its Cython kernels compiled from
+source into oracle/_ref) with its every-5th log-likelihood check, on a 25,000-row SNP
+slice of the same cohort, scaled linearly to the full M.
+``--impl reference`` prints the reference arm: that CPU implementation as the headline,
+each step on one of two 25,000-row slices (50,000 rows in all).
 """
 from __future__ import annotations
 
@@ -56,6 +64,7 @@ CONFIGS = {
                 N=200_000, M=50_000, K=10, F=0.02, alpha=((0.7, 0.05), (0.3, 1.0)), miss=0.01, seed=2000),
 }
 TC_PRECISIONS = ("bf16", "f16")   # the tensor-core sweep
+FP64_NOMINAL_TFLOPS = 40.0        # B200 float64 (vector and tensor core), NVIDIA's datasheet
 CHECK = 5
 HP = dict(lr=0.005, beta1=0.80, beta2=0.88, eps=1e-8)
 
@@ -138,63 +147,106 @@ class Clocks:
 
 # ---------------------------------------------------------------- CPU (reference) arm
 
-def cpu_reference_sample(cfg, coh, sample_snps, steps, warmup, G_rows=None):
-    """Time the reference's own Adam-EM CPU step (``adamStep``: em.P_step, em.Q_step,
-    em.adamUpdateP/Q; adamixture/model/em_adam.py:12-54) on the first ``sample_snps``
-    SNP rows of the cohort, all host cores. Returns (seconds per full-M iteration, info)."""
+REF_SLICE_ROWS = 25_000   # SNP rows per timed reference step
+REF_SLICES = 2            # the reference arm alternates over this many slices (50,000 rows)
+
+
+def cpu_reference_sample(cfg, slices, steps, warmup):
+    """Time the reference's own Adam-EM CPU iteration on SNP-row slices of the cohort, all
+    host cores: ``adamStep`` (em.P_step, em.Q_step, em.adamUpdateP/Q;
+    adamixture/model/em_adam.py:12-54) and, every 5th step, its log-likelihood check
+    (tools.loglikelihood; em_adam.py:136-160), the same step the GPU arm times. Step s runs
+    on ``slices[s % len(slices)]``. A step's full-M time scales the SNP-side work (P_step,
+    adamUpdateP, the check) by M / slice rows; the sample-side work (Q_step, adamUpdateQ)
+    does not depend on M and is counted once. Returns (seconds per full-M iteration, info)."""
     cores = os.cpu_count() or 1
     os.environ["OMP_NUM_THREADS"] = str(cores)
     from oracle import refmods  # the compiled reference kernels (test/baseline infrastructure)
 
     kind = "reference" if refmods.available() else "port"
     N, K, M = cfg["N"], cfg["K"], cfg["M"]
-    Ms = min(sample_snps, M)
-    if G_rows is None:
-        G_rows = np.empty((Ms, N), dtype=np.uint8)
-        blk = max(4, (1 << 24) // max(N, 1))
-        for s in range(0, Ms, blk):
-            G_rows[s:s + blk] = coh.genotypes(s, min(blk, Ms - s))
     rng = np.random.default_rng(cfg["seed"])
-    P = np.clip(rng.random((Ms, K)), 1e-5, 1 - 1e-5)
     Q = np.clip(rng.random((N, K)), 1e-5, 1 - 1e-5)
     Q /= Q.sum(1, keepdims=True)
+    states = []
+    for G_rows in slices:
+        Ms = G_rows.shape[0]
+        P = np.clip(rng.random((Ms, K)), 1e-5, 1 - 1e-5)
+        states.append(dict(G=G_rows, Ms=Ms, P=P, P1=np.zeros_like(P), mP=np.zeros_like(P),
+                           vP=np.zeros_like(P)))
     T = np.zeros_like(Q)
-    P1 = np.zeros_like(P)
     Q1 = np.zeros_like(Q)
     qb = np.zeros(N)
-    mP, vP, mQ, vQ = (np.zeros_like(P), np.zeros_like(P), np.zeros_like(Q), np.zeros_like(Q))
+    mQ, vQ = np.zeros_like(Q), np.zeros_like(Q)
     t = [0]
     if kind == "reference":
         em = refmods.load("em")
+        tools = refmods.load("tools")
 
-        def step():
-            em.P_step(G_rows, P, P1, Q, T, qb, K, Ms, N)
+        def step(st, check):
+            a = time.perf_counter()
+            em.P_step(st["G"], st["P"], st["P1"], Q, T, qb, K, st["Ms"], N)
+            b = time.perf_counter()
             em.Q_step(Q, Q1, T, qb, K, N)
             t[0] += 1
-            em.adamUpdateP(P, P1, mP, vP, HP["lr"], HP["beta1"], HP["beta2"], HP["eps"], t[0], Ms, K)
+            c = time.perf_counter()
+            em.adamUpdateP(st["P"], st["P1"], st["mP"], st["vP"], HP["lr"], HP["beta1"], HP["beta2"],
+                           HP["eps"], t[0], st["Ms"], K)
+            d = time.perf_counter()
             em.adamUpdateQ(Q, Q1, mQ, vQ, HP["lr"], HP["beta1"], HP["beta2"], HP["eps"], t[0], N, K)
+            e = time.perf_counter()
+            chk = 0.0
+            if check:
+                f0 = time.perf_counter()
+                tools.loglikelihood(st["G"], st["P"], Q)
+                chk = time.perf_counter() - f0
+            return (b - a) + (d - c), (c - b) + (e - d), chk
         threads = cores
     else:
         from oracle import em_oracle as orc
-        st = orc.Adam(HP["lr"], HP["beta1"], HP["beta2"], HP["eps"]).init(P, Q)
+        ad = orc.Adam(HP["lr"], HP["beta1"], HP["beta2"], HP["eps"]).init(states[0]["P"], Q)
 
-        def step():
-            A, B, Tt, q = orc.em_stats(G_rows, P, Q)
-            orc.adam_step(st, P, Q, *orc.em_final(P, Q, A, B, Tt, q))
+        def step(st, check):
+            a = time.perf_counter()
+            A, B, Tt, q = orc.em_stats(st["G"], st["P"], Q)
+            orc.adam_step(ad, st["P"], Q, *orc.em_final(st["P"], Q, A, B, Tt, q))
+            snp = time.perf_counter() - a
+            chk = 0.0
+            if check:
+                f0 = time.perf_counter()
+                orc.loglik(st["G"], st["P"], Q)
+                chk = time.perf_counter() - f0
+            return snp, 0.0, chk
         threads = 1
-    for _ in range(warmup):
-        step()
-    times = []
-    for _ in range(steps):
-        t0 = time.perf_counter()
-        step()
-        times.append(time.perf_counter() - t0)
-    per = float(np.median(times))
-    full = per * (M / Ms)
+    for it in range(warmup):
+        step(states[it % len(states)], (it + 1) % CHECK == 0)
+    full, sl = [], []
+    for it in range(steps):
+        st = states[it % len(states)]
+        snp, smp, chk = step(st, (it + 1) % CHECK == 0)
+        full.append((snp + chk) * (M / st["Ms"]) + smp)
+        sl.append(snp + smp + chk)
+    if steps < CHECK:
+        # too few steps for a check among them: one check, timed on its own, counts as
+        # 1/CHECK of a check per step
+        chk = step(states[0], True)[2]
+        full = [f + chk * (M / states[0]["Ms"]) / CHECK for f in full]
+        sl = [x + chk / CHECK for x in sl]
+    per = float(np.mean(full))
+    rows = sum(st["Ms"] for st in states)
     info = {"kind": kind, "cores": threads,
-            "sample": f"{Ms} of {M} SNP rows x all {N} samples, K={K}; median of {steps} adamStep "
-                      f"calls, scaled x{M / Ms:.1f} to the full M (cost is linear in M)"}
-    return full, info
+            "sample": f"{len(states)} slice(s) of {states[0]['Ms']} SNP rows ({rows} of {M} rows in all) x all "
+                      f"{N} samples, K={K}; step s on slice s mod {len(states)}; mean of {steps} reference "
+                      f"Adam-EM steps (adamStep + the log-likelihood check every {CHECK}th step), SNP-side "
+                      f"time scaled x{M / states[0]['Ms']:.1f} to the full M (its cost is linear in M)",
+            "timed_slice_ms": 1e3 * float(np.mean(sl)), "scale": M / states[0]["Ms"], "sample_rows": rows}
+    return per, info
+
+
+def host_slices(coh, M, n_slices, rows):
+    """The cohort's first ``n_slices * rows`` SNP rows, unpacked, sampled on the host."""
+    rows = min(rows, max(4, M // n_slices))
+    return [coh.genotypes_parallel(s * rows, rows) for s in range(n_slices)]
 
 
 def run_reference_arm(args, cfg, rank):
@@ -203,14 +255,15 @@ def run_reference_arm(args, cfg, rank):
     from adamixture_b200.src.simulate import make_cohort
 
     coh = make_cohort(cfg["N"], cfg["M"], cfg["K"], cfg["F"], cfg["alpha"], cfg["miss"], cfg["seed"])
-    sample = max(64, min(cfg["M"], int(args.cpu_snps)))
-    full, info = cpu_reference_sample(cfg, coh, sample, args.steps, args.warmup)
+    slices = host_slices(coh, cfg["M"], REF_SLICES, int(args.cpu_snps))
+    full, info = cpu_reference_sample(cfg, slices, args.steps, args.warmup)
     v = 1.0 / full
     line = {
         "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": full * 1e3,
         "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic", "config": {"workload": cfg["workload"], "sample_snps": sample},
+        "data": "synthetic", "config": {"workload": cfg["workload"], "sample_rows": info["sample_rows"],
+                                        "check_every": CHECK},
         "cpu_baseline": dict(value=v, unit=UNIT, **info),
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -219,43 +272,23 @@ def run_reference_arm(args, cfg, rank):
 
 # ---------------------------------------------------------------- GPU arm
 
-def run_gpu_arm(args, cfg, rank, world, local_rank):
+def _sweep_kernel_name(prec, K):
+    if prec in TC_PRECISIONS:
+        return f"em_sweep_tc_kernel<{prec == 'f16'}>"
+    return f"em_sweep_kernel<{'double' if prec == 'f64' else 'float'},{ops_kmax(K)}>"
+
+
+def time_steps(prec, G, P0, Q0, M_loc, N, K, dev, steps, warmup, sharded, clocks=None):
+    """Adam-EM steps at one E-step arithmetic from (P0, Q0): ``warmup`` untimed steps, then
+    ``steps`` steps between CUDA events on the launching stream (barrier + synchronize on
+    both sides, max over ranks when sharded). Returns the step time, the kernel launches of
+    the timed region and the final P/Q (for the sweep's roofline)."""
     import torch
 
     from adamixture_b200 import ops
-    from adamixture_b200.model.em_adam_gpu import EMAdamOptimizer, optimize_parameters_gpu, resolve_precision
-    from adamixture_b200.src.simulate import make_cohort
+    from adamixture_b200.model.em_adam_dist import CudaBackend, ShardedAdamEM
+    from adamixture_b200.model.em_adam_gpu import EMAdamOptimizer
 
-    dev = torch.device("cuda", local_rank)
-    torch.cuda.set_device(dev)
-    N, M, K = cfg["N"], cfg["M"], cfg["K"]
-    prec = resolve_precision(K, args.precision)
-    sharded = world > 1 or args.shard
-    if sharded:
-        import datetime
-
-        import torch.distributed as dist
-        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
-        os.environ.setdefault("MASTER_PORT", "29531")
-        os.environ.setdefault("RANK", str(rank))
-        os.environ.setdefault("WORLD_SIZE", str(world))
-        dist.init_process_group("nccl", device_id=dev, timeout=datetime.timedelta(minutes=10))
-
-    from adamixture_b200.model.em_adam_dist import CudaBackend, ShardedAdamEM, shard_rows
-    from adamixture_b200.src.simulate import shard_keys
-
-    coh = make_cohort(N, M, K, cfg["F"], cfg["alpha"], cfg["miss"], cfg["seed"])
-    # this rank's SNP rows (all of them on one GPU); exactly that slice of the cohort
-    j0, j1 = shard_rows(M, world, rank) if world > 1 else (0, M)
-    M_loc = j1 - j0
-    Pq = torch.from_numpy(coh.Pq[j0:j1].astype(np.int32)).to(dev)
-    Qq = torch.from_numpy(coh.Qq.astype(np.int32)).to(dev)
-    G = ops.simulate_packed(Pq, Qq, coh.miss_q, shard_keys(coh.keys, j0, N))
-    del Pq, Qq
-    rng = np.random.default_rng(cfg["seed"])
-    P0 = np.clip(rng.random((M, K)), 1e-5, 1 - 1e-5)[j0:j1].copy()
-    Q0 = np.clip(rng.random((N, K)), 1e-5, 1 - 1e-5)
-    Q0 /= Q0.sum(1, keepdims=True)
     P = torch.from_numpy(P0).to(dev)
     Q = torch.from_numpy(Q0).to(dev)
     P32, Q32 = P.float(), Q.float()
@@ -263,18 +296,17 @@ def run_gpu_arm(args, cfg, rank, world, local_rank):
     llp = "f64" if prec == "f64" else "f32"
     Pll, Qll = (P, Q) if llp == "f64" else (P32, Q32)
     launches = {"n": 0}
-
     if not sharded:
-        # kernels per fused iteration: sweep (+ the BF16 copy of Q for the tensor-core sweep)
-        # and the update kernel; per check: the log-likelihood kernel and its final sum
+        # kernels per fused iteration: sweep (+ the 16-bit copy of Q for the tensor-core
+        # sweep) and the update kernel; per check: the log-likelihood kernel and its final sum
         opt = EMAdamOptimizer(P.shape, Q.shape, HP["lr"], HP["beta1"], HP["beta2"], HP["eps"], dev, prec)
         per_iter = 3 if prec in TC_PRECISIONS else 2
 
         def one_step(it):
-            opt.fused_iteration(G, P, Q, P32, Q32, M, ws)
+            opt.fused_iteration(G, P, Q, P32, Q32, M_loc, ws)
             launches["n"] += per_iter
             if (it + 1) % CHECK == 0:
-                float(ops.loglik_device(G, Pll, Qll, M, llp).item())
+                float(ops.loglik_device(G, Pll, Qll, M_loc, llp).item())
                 launches["n"] += 2
     else:
         # SNP-sharded: local sweep + statistics, all-reduce of T, targets, Adam (Q replicated)
@@ -290,36 +322,44 @@ def run_gpu_arm(args, cfg, rank, world, local_rank):
                 launches["n"] += 2
 
     torch.cuda.synchronize()
-    for it in range(args.warmup):
+    for it in range(warmup):
         one_step(it)
     torch.cuda.synchronize()
     launches["n"] = 0
     if sharded:
         torch.distributed.barrier()
     torch.cuda.synchronize()
-    uuid = None
-    try:
-        uuid = "GPU-" + str(torch.cuda.get_device_properties(dev).uuid)
-    except Exception:
-        pass
     stream = torch.cuda.current_stream(dev)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with Clocks(uuid) as clk:
+    import contextlib
+    with (clocks if clocks is not None else contextlib.nullcontext()):
         e0.record(stream)
-        for it in range(args.steps):
+        for it in range(steps):
             one_step(it)
         e1.record(stream)
         torch.cuda.synchronize()
     ms = e0.elapsed_time(e1)
     if sharded:
+        torch.distributed.barrier()
         t = torch.tensor([ms], device=dev)
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         ms = float(t.item())
-    ms_per_step = ms / args.steps
+    if ops.em_status(ws, M_loc, N, K, prec) != 0:
+        raise RuntimeError(f"E-step sweep reported a nonzero status ({prec})")
+    return {"ms_per_step": ms / steps, "launches": launches["n"], "P": P, "Q": Q}
 
-    # roofline: the sweep kernel alone (this rank's rows), CUDA events on its stream
+
+def sweep_roofline(prec, G, P, Q, M_loc, N, K, dev, reps):
+    """The E-step sweep kernel alone (this rank's rows): mean of ``reps`` launches between
+    CUDA events on its stream, after one warm-up launch; algorithmic bytes per launch
+    ceil(M/4) N + 4K(3M+2N) against the measured HBM copy bandwidth."""
+    import torch
+
+    from adamixture_b200 import ops
+
     Pin, Qin = (P, Q) if prec == "f64" else (P.float(), Q.float())
-    reps = max(3, min(10, args.steps))
+    ws = ops.Workspace.get(dev, ops.em_workspace_bytes(M_loc, N, K, prec))
+    stream = torch.cuda.current_stream(dev)
     ops.em_sweep(G, Pin, Qin, M_loc, prec, ws)
     torch.cuda.synchronize()
     s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -334,20 +374,91 @@ def run_gpu_arm(args, cfg, rank, world, local_rank):
     achieved = ab / (sweep_ms * 1e-3) / 1e9
     roof = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
             "frac": achieved / hbm, "traffic": traffic_per_launch(M_loc, N, K, prec),
-            "kernel": f"em_sweep_tc_kernel<{prec == 'f16'}>" if prec in TC_PRECISIONS else f"em_sweep_kernel<{'double' if prec == 'f64' else 'float'},{ops_kmax(K)}>",
-            "launch_ms": sweep_ms, "alg_bytes": ab, "peak_kind": peak_kind,
-            "entries_per_s": M_loc * N / (sweep_ms * 1e-3), "snp_rows_per_rank": M_loc}
+            "kernel": _sweep_kernel_name(prec, K), "launch_ms": sweep_ms, "alg_bytes": ab,
+            "peak_kind": peak_kind, "entries_per_s": M_loc * N / (sweep_ms * 1e-3),
+            "snp_rows_per_rank": M_loc}
+    flops = 8.0 * M_loc * N * K
     if prec in TC_PRECISIONS:
         # the contractions (h, 1-h, A, B, T: 8 M N K flops of useful work; K padded to 16 in
-        # the MMAs) against the measured dense BF16 peak (FP16's dense rate is the same), for
-        # the tensor-core sweep
+        # the MMAs) against the measured dense BF16 peak (FP16's dense rate is the same)
         tf = peaks_tensor()
-        flops = 8.0 * M_loc * N * K
         roof["tensor"] = {"achieved_tflops": flops / (sweep_ms * 1e-3) / 1e12, "peak_tflops": tf,
                           "frac": flops / (sweep_ms * 1e-3) / 1e12 / tf if tf else None,
                           "flops_per_launch": flops}
+    elif prec == "f64":
+        # the same contractions in float64, against B200's nominal float64 rate (no measured
+        # float64 peak exists for this pool)
+        roof["fp64"] = {"achieved_tflops": flops / (sweep_ms * 1e-3) / 1e12,
+                        "peak_tflops": FP64_NOMINAL_TFLOPS, "peak_kind": "nominal",
+                        "frac": flops / (sweep_ms * 1e-3) / 1e12 / FP64_NOMINAL_TFLOPS,
+                        "flops_per_launch": flops}
+    return roof
 
-    # e2e through the public API from pinned host buffers
+
+def run_gpu_arm(args, cfg, rank, world, local_rank):
+    import torch
+
+    from adamixture_b200 import ops
+    from adamixture_b200.model.em_adam_gpu import resolve_precision
+    from adamixture_b200.src.simulate import make_cohort
+
+    dev = torch.device("cuda", local_rank)
+    torch.cuda.set_device(dev)
+    N, M, K = cfg["N"], cfg["M"], cfg["K"]
+    prec = resolve_precision(K, args.precision or "f64")
+    sharded = world > 1 or args.shard
+    if sharded:
+        import datetime
+
+        import torch.distributed as dist
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        os.environ.setdefault("MASTER_PORT", "29531")
+        os.environ.setdefault("RANK", str(rank))
+        os.environ.setdefault("WORLD_SIZE", str(world))
+        dist.init_process_group("nccl", device_id=dev, timeout=datetime.timedelta(minutes=10))
+
+    from adamixture_b200.model.em_adam_dist import shard_rows
+    from adamixture_b200.src.simulate import shard_keys
+
+    coh = make_cohort(N, M, K, cfg["F"], cfg["alpha"], cfg["miss"], cfg["seed"])
+    # this rank's SNP rows (all of them on one GPU); exactly that slice of the cohort
+    j0, j1 = shard_rows(M, world, rank) if world > 1 else (0, M)
+    M_loc = j1 - j0
+    Pq = torch.from_numpy(coh.Pq[j0:j1].astype(np.int32)).to(dev)
+    Qq = torch.from_numpy(coh.Qq.astype(np.int32)).to(dev)
+    G = ops.simulate_packed(Pq, Qq, coh.miss_q, shard_keys(coh.keys, j0, N))
+    del Pq, Qq
+    rng = np.random.default_rng(cfg["seed"])
+    P0 = np.clip(rng.random((M, K)), 1e-5, 1 - 1e-5)[j0:j1].copy()
+    Q0 = np.clip(rng.random((N, K)), 1e-5, 1 - 1e-5)
+    Q0 /= Q0.sum(1, keepdims=True)
+
+    uuid = None
+    try:
+        uuid = "GPU-" + str(torch.cuda.get_device_properties(dev).uuid)
+    except Exception:
+        pass
+    clk = Clocks(uuid)
+    head = time_steps(prec, G, P0, Q0, M_loc, N, K, dev, args.steps, args.warmup, sharded, clocks=clk)
+    ms_per_step = head["ms_per_step"]
+    reps = max(3, min(10, args.steps))
+    roof = sweep_roofline(prec, G, head["P"], head["Q"], M_loc, N, K, dev, reps)
+    del head["P"], head["Q"]
+
+    # the other E-step arithmetics from the same start, each with its own sweep roofline
+    variants = {}
+    if not args.no_variants:
+        for vp in ("f32", "f16", "bf16"):
+            if vp == prec or (vp in TC_PRECISIONS and K > 16):
+                continue
+            r = time_steps(vp, G, P0, Q0, M_loc, N, K, dev, args.steps, args.warmup, sharded)
+            variants[vp] = {"value": 1000.0 / r["ms_per_step"], "unit": UNIT, "ms_per_step": r["ms_per_step"],
+                            "dtype": vp, "gpu_launches": r["launches"],
+                            "roofline": sweep_roofline(vp, G, r["P"], r["Q"], M_loc, N, K, dev, reps)}
+            del r
+        torch.cuda.synchronize()
+
+    # e2e through the public API from pinned host buffers, at the headline arithmetic
     e2e = None
     if not args.no_e2e:
         if not sharded:
@@ -355,10 +466,16 @@ def run_gpu_arm(args, cfg, rank, world, local_rank):
         else:
             e2e = run_e2e_dist(args, G, P0, Q0, M_loc, N, K, prec, dev, world)
 
+    # whole fits to the converged log-likelihood (one GPU)
+    ttt = None
+    if not args.no_converge and not sharded:
+        ttt = converge_runs(args, cfg, G, dev, ("f32", "f16", "warm_f16"))
+
     cpu = None
     if not args.no_cpu and rank == 0 and world == 1:
-        G_rows = ops.unpack_u8(G, 0, min(M, args.cpu_snps), M).cpu().numpy()
-        full, info = cpu_reference_sample(cfg, coh, min(M, args.cpu_snps), 3, 1, G_rows=G_rows)
+        rows = min(M, int(args.cpu_snps))
+        G_rows = ops.unpack_u8(G, 0, rows, M).cpu().numpy()
+        full, info = cpu_reference_sample(cfg, [G_rows], 2, 0)
         cpu = dict(value=1.0 / full, unit=UNIT, **info)
 
     if rank == 0:
@@ -366,15 +483,15 @@ def run_gpu_arm(args, cfg, rank, world, local_rank):
             "metric": METRIC, "value": 1000.0 / ms_per_step, "unit": UNIT,
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "strong",
-            "vs_baseline": None, "dtype": {"f64": "f64", "f32": "f32", "bf16": "bf16", "f16": "f16"}[prec],
-            "data": "synthetic",
+            "vs_baseline": None, "dtype": prec, "data": "synthetic",
             "config": {"workload": cfg["workload"], "precision": prec, "check_every": CHECK,
                        "l2": "inputs (packed G) larger than L2; no flush",
                        "genotype_GBps": ((M + 3) // 4) * N / (ms_per_step * 1e-3) / 1e9,
                        "parallelism": "single GPU" if not sharded else
                        f"SNP rows sharded over {world} rank(s) (one all-reduce of T per iteration)"},
-            "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
-            "gpu_launches": launches["n"], "clocks": clk.summary(),
+            "roofline": roof, "variants": variants, "time_to_target": ttt,
+            "cpu_baseline": cpu, "e2e": e2e,
+            "gpu_launches": head["launches"], "clocks": clk.summary(),
         }
         print(json.dumps(line), flush=True)
     if sharded:
@@ -580,37 +697,33 @@ def run_kernels(args, cfg):
     print(json.dumps(line), flush=True)
 
 
-def run_converge(args, cfg):
-    """Time to the converged log-likelihood at the config: from the reference's default
-    start (randomized SVD + ALS), plain float32 Adam-EM to its stop, then the BF16 and FP16
-    tensor-core sweeps, mixed (tensor-core then float32) and the learned warm start with
-    the default arithmetic, each timed to the first check within 1e-6 relative of the plain
-    float32 run's best log-likelihood. One JSON line."""
+CONVERGE_RUNS = ("f32", "bf16", "f16", "mixed", "warm_f16")
+
+
+def converge_runs(args, cfg, G, dev, which=CONVERGE_RUNS):
+    """Time to the converged log-likelihood on the resident cohort G: from the reference's
+    default start (randomized SVD + ALS, seed 42), plain float32 Adam-EM to its stop, then
+    the other runs in ``which`` (BF16 / FP16 tensor-core sweeps, mixed: tensor-core then
+    float32, warm_f16: the learned warm start in front of the FP16 sweep), each timed to
+    the first check within 1e-6 relative of the plain float32 run's best log-likelihood."""
     import torch
 
-    from adamixture_b200 import ops
     from adamixture_b200.model import warm_start as ws
     from adamixture_b200.model.em_adam_gpu import loglikelihood_gpu, optimize_parameters_gpu
-    from adamixture_b200.src.simulate import make_cohort
 
-    dev = torch.device("cuda", 0)
     N, M, K = cfg["N"], cfg["M"], cfg["K"]
-    coh = make_cohort(N, M, K, cfg["F"], cfg["alpha"], cfg["miss"], cfg["seed"])
-    Pq = torch.from_numpy(coh.Pq.astype(np.int32)).to(dev)
-    Qq = torch.from_numpy(coh.Qq.astype(np.int32)).to(dev)
-    G = ops.simulate_packed(Pq, Qq, coh.miss_q, coh.keys)
-    del Pq, Qq
+    tc = 8 <= K <= 16
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     U, S, V, P0, Q0 = ws.init_als(G, N, M, K, seed=42)
     torch.cuda.synchronize()
     t_init = time.perf_counter() - t0
     runs = {}
+    precs = {"f32": "f32", "bf16": "bf16" if tc else "f32", "f16": "f16" if tc else "f32",
+             "mixed": "mixed", "warm_f16": "f16" if tc else "f32"}
     # load every kernel instance the fits use before any of them is timed (the first
     # launch of a kernel loads its module)
-    for prec in ("f32", "bf16", "f16"):
-        if prec in TC_PRECISIONS and K > 16:
-            continue
+    for prec in sorted({precs[w] for w in which} | {"f32"}):
         optimize_parameters_gpu(G, P0.clone(), Q0.clone(), HP["lr"], HP["beta1"], HP["beta2"], HP["eps"],
                                 CHECK, CHECK, K, M, N, 0.5, 1e-4, 3, 0.1, dev, 8192, 256, precision=prec)
     loglikelihood_gpu(G, P0, Q0, M, N, 8192, dev, 256)
@@ -627,32 +740,115 @@ def run_converge(args, cfg):
         el = time.perf_counter() - t
         L = loglikelihood_gpu(G, P, Q, M, N, 8192, dev, 256)
         runs[name] = {"precision": prec, "seconds": el + extra_s, "iterations": tr[-1][0] if tr else 0,
-                      "loglik": L, "trace": tr}
+                      "loglik": L, "trace": [(it, Lc, sec + extra_s) for it, Lc, sec in tr],
+                      "extra_seconds": extra_s}
 
-    fit("plain_f32", P0, Q0, "f32")
-    target = max(e[1] for e in runs["plain_f32"]["trace"])
-    fit("bf16", P0, Q0, "bf16" if 8 <= K <= 16 else "f32")
-    fit("f16", P0, Q0, "f16" if 8 <= K <= 16 else "f32")
-    fit("mixed", P0, Q0, "mixed")
-    net = ws.WarmStartMLP.load(ws.DEFAULT_WEIGHTS, dev)
-    torch.cuda.synchronize()
-    t = time.perf_counter()
-    Pw, Qw = ws.predict(net, G, M, U, S, V, Q0, P0)
-    torch.cuda.synchronize()
-    fit("warm_auto", Pw, Qw, "auto", extra_s=time.perf_counter() - t)
+    fit("f32", P0, Q0, "f32")
+    target = max(e[1] for e in runs["f32"]["trace"])
+    for w in which:
+        if w in ("f32", "warm_f16"):
+            continue
+        fit(w, P0, Q0, precs[w])
+    if "warm_f16" in which:
+        net = ws.WarmStartMLP.load(ws.DEFAULT_WEIGHTS, dev)
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        Pw, Qw = ws.predict(net, G, M, U, S, V, Q0, P0)
+        torch.cuda.synchronize()
+        fit("warm_f16", Pw, Qw, precs["warm_f16"], extra_s=time.perf_counter() - t)
     out = {}
+    base = runs["f32"]
+    base_reach = next(((it, sec) for it, L, sec in base["trace"] if L >= target - 1e-6 * abs(target)), None)
     for name, r in runs.items():
         reach = next(((it, sec) for it, L, sec in r["trace"] if L >= target - 1e-6 * abs(target)), None)
-        out[name] = {"precision": r["precision"], "seconds_to_stop": r["seconds"], "iterations_to_stop": r["iterations"],
-                     "loglik": r["loglik"], "rel_gap_to_plain_f32": (runs["plain_f32"]["loglik"] - r["loglik"])
-                     / abs(runs["plain_f32"]["loglik"]),
+        out[name] = {"precision": r["precision"], "seconds_to_target": reach[1] if reach else None,
                      "iterations_to_target": reach[0] if reach else None,
-                     "seconds_to_target": reach[1] if reach else None}
-    line = {"metric": "time-to-converged loglik", "config": {"workload": cfg["workload"],
-            "start": "randomized SVD (k=max(K,16), power 5) + ALS, seed 42", "check_every": CHECK,
-            "max_iter": args.converge_max_iter, "target": "first check within 1e-6 relative of the plain float32 "
-            "run's best (traced) log-likelihood"}, "init_seconds": t_init, "runs": out}
-    print(json.dumps(line), flush=True)
+                     "frac_of_f32_time": (reach[1] / base_reach[1]) if (reach and base_reach) else None,
+                     "seconds_to_stop": r["seconds"], "iterations_to_stop": r["iterations"],
+                     "loglik": r["loglik"],
+                     "rel_gap_to_f32": (base["loglik"] - r["loglik"]) / abs(base["loglik"])}
+        if r["extra_seconds"]:
+            out[name]["warm_start_seconds"] = r["extra_seconds"]
+    return {"target": "first check within 1e-6 relative of the plain float32 run's best (traced) "
+                      "log-likelihood; seconds are wall time of optimize_parameters_gpu on the resident "
+                      "cohort (warm_f16 includes the network's prediction)",
+            "start": "randomized SVD (k=max(K,16), power 5) + ALS, seed 42", "init_seconds": t_init,
+            "check_every": CHECK, "max_iter": args.converge_max_iter, "target_loglik": target,
+            "runs": out}
+
+
+def run_converge(args, cfg):
+    """``--converge``: the time-to-target runs of every arithmetic as one JSON line."""
+    import torch
+
+    from adamixture_b200 import ops
+    from adamixture_b200.src.simulate import make_cohort
+
+    dev = torch.device("cuda", 0)
+    N, M, K = cfg["N"], cfg["M"], cfg["K"]
+    coh = make_cohort(N, M, K, cfg["F"], cfg["alpha"], cfg["miss"], cfg["seed"])
+    Pq = torch.from_numpy(coh.Pq.astype(np.int32)).to(dev)
+    Qq = torch.from_numpy(coh.Qq.astype(np.int32)).to(dev)
+    G = ops.simulate_packed(Pq, Qq, coh.miss_q, coh.keys)
+    del Pq, Qq
+    res = converge_runs(args, cfg, G, dev)
+    print(json.dumps({"metric": "time-to-converged loglik", "config": {"workload": cfg["workload"]}, **res}),
+          flush=True)
+
+
+def run_errors(args, cfg):
+    """``--errors``: each E-step arithmetic against the float64 run of the same iterations.
+    From the benchmark's start (P0, Q0), the priming step and ``--error-iters`` iterations
+    in float64, float32, FP16 and BF16 (tensor-core forms where K <= 16); after each
+    iteration, max |P - P_f64|, max |Q - Q_f64| and the float64 log-likelihood's relative
+    gap to the float64 run's. One JSON line."""
+    import torch
+
+    from adamixture_b200 import ops
+    from adamixture_b200.model.em_adam_gpu import EMAdamOptimizer
+    from adamixture_b200.src.simulate import make_cohort
+
+    dev = torch.device("cuda", 0)
+    N, M, K = cfg["N"], cfg["M"], cfg["K"]
+    coh = make_cohort(N, M, K, cfg["F"], cfg["alpha"], cfg["miss"], cfg["seed"])
+    G = ops.simulate_packed(torch.from_numpy(coh.Pq.astype(np.int32)).to(dev),
+                            torch.from_numpy(coh.Qq.astype(np.int32)).to(dev), coh.miss_q, coh.keys)
+    rng = np.random.default_rng(cfg["seed"])
+    P0 = np.clip(rng.random((M, K)), 1e-5, 1 - 1e-5)
+    Q0 = np.clip(rng.random((N, K)), 1e-5, 1 - 1e-5)
+    Q0 /= Q0.sum(1, keepdims=True)
+    n = args.error_iters
+    ref = []
+    out = {}
+    for prec in ("f64", "f32", "f16", "bf16"):
+        if prec in TC_PRECISIONS and K > 16:
+            continue
+        P = torch.from_numpy(P0).to(dev)
+        Q = torch.from_numpy(Q0).to(dev)
+        P32, Q32 = P.float(), Q.float()
+        ws = ops.Workspace.get(dev, ops.em_workspace_bytes(M, N, K, prec))
+        opt = EMAdamOptimizer(P.shape, Q.shape, HP["lr"], HP["beta1"], HP["beta2"], HP["eps"], dev, prec)
+        rows = []
+        for it in range(n + 1):
+            opt.fused_iteration(G, P, Q, P32, Q32, M, ws)
+            L = float(ops.loglik_device(G, P, Q, M, "f64").item())
+            if prec == "f64":
+                ref.append((P.clone(), Q.clone(), L))
+                rows.append({"iteration": it, "loglik": L})
+            else:
+                Pr, Qr, Lr = ref[it]
+                rows.append({"iteration": it, "max_abs_dP": float((P - Pr).abs().max()),
+                             "max_abs_dQ": float((Q - Qr).abs().max()),
+                             "rel_loglik_gap": (Lr - L) / abs(Lr), "loglik": L})
+        if ops.em_status(ws, M, N, K, prec) != 0:
+            raise RuntimeError(f"E-step sweep reported a nonzero status ({prec})")
+        out[prec] = rows
+        del P, Q, P32, Q32, opt
+        torch.cuda.synchronize()
+    print(json.dumps({"metric": "E-step arithmetic error against float64", "config": {
+        "workload": cfg["workload"], "start": "reference random EM start, default_rng(seed)",
+        "iterations": "0 = after the priming step; then Adam-EM iterations",
+        "loglik": "float64 log-likelihood of each run's own P, Q"}, "runs": out}), flush=True)
 
 
 def run_e2e_dist(args, G_dev, P0, Q0, M_loc, N, K, prec, dev, world):
@@ -698,15 +894,23 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--precision", default=None)
     ap.add_argument("--config", choices=sorted(CONFIGS), default="c3")
-    ap.add_argument("--cpu-snps", dest="cpu_snps", type=int, default=4096)
+    ap.add_argument("--cpu-snps", dest="cpu_snps", type=int, default=REF_SLICE_ROWS,
+                    help="SNP rows per timed reference step")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-variants", dest="no_variants", action="store_true",
+                    help="skip the float32 / FP16 / BF16 variant measurements")
+    ap.add_argument("--no-converge", dest="no_converge", action="store_true",
+                    help="skip the time-to-target fits")
     ap.add_argument("--shard", action="store_true",
                     help="use the SNP-sharded path (NCCL all-reduce of T) even on one GPU")
     ap.add_argument("--converge", action="store_true",
                     help="instead of the throughput line, time runs to the converged log-likelihood")
     ap.add_argument("--converge-max-iter", dest="converge_max_iter", type=int, default=300)
     ap.add_argument("--kernels", action="store_true", help="per-kernel timings at the config's shape")
+    ap.add_argument("--errors", action="store_true",
+                    help="per-iteration error of each E-step arithmetic against the float64 run")
+    ap.add_argument("--error-iters", dest="error_iters", type=int, default=20)
     ap.add_argument("--kernels-skip-hessian", dest="kernels_skip_hessian", action="store_true")
     ap.add_argument("--sweep-by-k", dest="sweep_by_k", action="store_true",
                     help="float32 vs FP16 tensor-core sweep time for K = 2..16")
@@ -728,6 +932,10 @@ def main():
     if args.kernels:
         if rank == 0:
             run_kernels(args, cfg)
+        return
+    if args.errors:
+        if rank == 0:
+            run_errors(args, cfg)
         return
     if args.sweep_by_k:
         if rank == 0:

@@ -159,7 +159,9 @@ int adx_loglik(const uint8_t* G, int64_t M, int64_t N, int K, int precision, con
  * workspace; every problem size fits (the plan never needs more than 1776 partials; the array holds
  * 2048, and a larger plan would be rejected with ADX_ERR_WORKSPACE).
  * The first call on a device (with it current) looks up the array's address; make it
- * before any stream capture. Calls share the array: calls that overlap on the GPU race.
+ * before any stream capture. The address stays cached for the process: after a
+ * cudaDeviceReset on that device this entry point must not be called there again.
+ * Calls share the array: calls that overlap on the GPU race.
  * Allocates nothing; *out is a device double. */
 int adx_loglik_noalloc(const uint8_t* G, int64_t M, int64_t N, int K, int precision,
                        const void* P, const void* Q, double* out, void* stream);

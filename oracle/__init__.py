@@ -12,8 +12,10 @@ Contents:
   file:line it follows.
 * ``refmods``: a loader for the reference's own Cython CPU kernels, which
   ``oracle/Makefile`` compiles from the reference sources into ``oracle/_ref/``.
-* ``synth``: the seeded synthetic-cohort generator restated on the CPU with exact
-  integer arithmetic, so that the CUDA generator can be checked bit for bit.
+* ``solvers``: float64 restatements of the per-row solvers (BVLS, the SQP active-set QP,
+  the simplex and box projections), the BR-QN gradient/Hessian sums, the randomized-SVD
+  products and the CV deviance.
+* ``mlp``: a float64 restatement of the warm-start network's forward and backward passes.
 
 Parity is pinned: ``tests/golden/make_golden.py`` runs the reference's own Python
 implementation (imported from the reference tree in the build container) and the

@@ -25,7 +25,10 @@ import types
 from pathlib import Path
 
 REF_DIR = Path(__file__).resolve().parent / "_ref"
-REFERENCE_TREE = Path(os.environ.get("ADX_REFERENCE_TREE", "/root/reference"))
+# The reference project tree: ADX_REFERENCE_TREE when set, else a sibling directory named
+# "reference" beside this repository's root.
+REFERENCE_TREE = Path(os.environ.get("ADX_REFERENCE_TREE",
+                                     Path(__file__).resolve().parent.parent.parent / "reference"))
 MODULES = ("em", "tools", "sqp", "bvls", "br_qn", "snp_reader", "clumppling")
 
 _loaded: dict[str, types.ModuleType] = {}

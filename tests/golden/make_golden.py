@@ -29,6 +29,13 @@ CUDA unpack op replaced by a bit-shift unpacker of the same packed layout):
 * ``align.npz``: the reference's cluster alignment across K on seeded Q matrices.
 * ``cv_proj.npz``: the reference's cross-validation index (5 folds, seed 42) and fold
   rules, and its Adam-EM and SQP + ZAL projections, on a seeded cohort (N=90, M=700, K=3).
+* ``c2_trace.npz`` (only when named: about 20 minutes on 8 cores): the reference's
+  Adam-EM iterations on the mid-size benchmark cohort (N=10,000, M=200,000, K=8,
+  Balding-Nichols F=0.05, Q Dirichlet(0.3), 0.5 % missing; the seeded sampler of
+  adamixture_b200/src/simulate.py, seed 1000) from the reference's random EM start
+  drawn with default_rng(1000): the priming step and 20 iterations, each recorded as P on
+  1,024 seeded SNP rows and Q on 1,024 seeded samples (float32) plus the column sums of
+  the full P and Q (float64), and the log-likelihood after iterations 0, 5, 10, 15, 20.
 """
 from __future__ import annotations
 
@@ -317,6 +324,59 @@ def align():
     print("align.npz", len(rec))
 
 
+C2 = dict(N=10_000, M=200_000, K=8, F=0.05, alpha=0.3, miss=0.005, seed=1000)
+
+
+def c2_cohort():
+    """The mid-size benchmark cohort (the same generator, parameters and seed as the
+    benchmark's c2 configuration) and its reference random start."""
+    from adamixture_b200.src.packing import pack
+    from adamixture_b200.src.simulate import make_cohort
+
+    c = C2
+    coh = make_cohort(c["N"], c["M"], c["K"], c["F"], c["alpha"], c["miss"], c["seed"])
+    rng = np.random.default_rng(c["seed"])
+    P0 = np.clip(rng.random((c["M"], c["K"])), 1e-5, 1 - 1e-5)
+    Q0 = np.clip(rng.random((c["N"], c["K"])), 1e-5, 1 - 1e-5)
+    Q0 /= Q0.sum(1, keepdims=True)
+    return coh, P0, Q0, pack
+
+
+def c2_trace(em, utils):
+    coh, P0, Q0, pack = c2_cohort()
+    M, N, K = coh.M, coh.N, coh.K
+    Gp = np.zeros(((M + 3) // 4, N), dtype=np.uint8)
+    blk = 8192
+    for s in range(0, M, blk):
+        g = coh.genotypes_parallel(s, min(blk, M - s))
+        Gp[s // 4: s // 4 + (g.shape[0] + 3) // 4] = pack(g)
+    sel = np.random.default_rng(7)
+    rows_P = np.sort(sel.choice(M, 1024, replace=False))
+    rows_Q = np.sort(sel.choice(N, 1024, replace=False))
+    dev = torch.device("cpu")
+    G = torch.from_numpy(Gp)
+    P = torch.from_numpy(P0.copy())
+    Q = torch.from_numpy(Q0.copy())
+    opt = em.EMAdamOptimizer(P.shape, Q.shape, HP["lr"], HP["beta1"], HP["beta2"], HP["reg_adam"], dev)
+    tP, tQ, sP, sQ, ll = [], [], [], [], {}
+    for it in range(21):
+        opt.run_em_step(G, P, Q, M, 8192, torch_unpacker)
+        opt.step(P, Q, opt.P_EM, opt.Q_EM)
+        Pn, Qn = P.numpy(), Q.numpy()
+        tP.append(Pn[rows_P].astype(np.float32))
+        tQ.append(Qn[rows_Q].astype(np.float32))
+        sP.append(Pn.sum(0))
+        sQ.append(Qn.sum(0))
+        if it % 5 == 0:
+            ll[it] = em.loglikelihood_gpu(G, P, Q, M, N, 8192, dev, 1)
+        print("c2 iteration", it, flush=True)
+    np.savez_compressed(OUT / "c2_trace.npz", N=N, M=M, K=K, seed=C2["seed"], rows_P=rows_P, rows_Q=rows_Q,
+                        trace_P=np.stack(tP), trace_Q=np.stack(tQ), colsum_P=np.stack(sP),
+                        colsum_Q=np.stack(sQ), loglik_iters=np.array(sorted(ll)),
+                        loglik=np.array([ll[k] for k in sorted(ll)]))
+    print("c2_trace.npz")
+
+
 if __name__ == "__main__":
     which = set(sys.argv[1:]) or {"edge", "synth", "demo", "demo_gpu", "solvers", "cv_proj", "align", "supervised"}
     if which & {"edge", "synth", "demo", "cv_proj", "supervised"}:
@@ -331,6 +391,9 @@ if __name__ == "__main__":
             cv_proj(em, utils)
         if "supervised" in which:
             supervised(em, utils)
+    if "c2" in which:
+        em, utils = reference()
+        c2_trace(em, utils)
     if "demo_gpu" in which:
         demo_gpu()
     if "solvers" in which:

@@ -142,7 +142,11 @@ def test_tc_converged_loglik(ops, prec, name, request):
     L = loglikelihood_gpu(G, P, Q, M, N, 8192, G.device, 512)
     ref = float(d["conv_loglik"])
     print(name, prec, "converged loglik", L, "reference", ref, "rel", abs(L - ref) / abs(ref))
-    assert abs(L - ref) <= 1e-4 * abs(ref)
+    # FP16 operands (the default): the 1e-6 relative bar of the converged fit (measured
+    # 1.2e-7 on demo, 7.4e-9 on synth). BF16 operands round 8x coarser; their bar is set
+    # at the measured gap (4.1e-6 on demo, 3.6e-7 on synth) with headroom, not at 1e-6.
+    bar = 1e-6 if prec == "f16" else 1e-5
+    assert abs(L - ref) <= bar * abs(ref)
 
 
 @pytest.mark.parametrize("name", ["demo", "synth"])
