@@ -396,6 +396,14 @@ int tc_sweep(const uint8_t* G, const float* P, const float* Q, int64_t M, int64_
              int64_t n_stile, int n_split, int n_mblk, float* ABp, float* Tp, void* Qb, int* err,
              bool f16, cudaStream_t st);
 
+int dmma_plan_width();
+int dmma_plan_chunk();
+int dmma_sweep(const uint8_t* G, const double* P, const double* Q, int64_t M, int64_t N, int K,
+               int64_t n_stile, int n_split, int n_mblk, int64_t mb, double* ABp, double* Tp,
+               cudaStream_t st);
+// Float64 sweeps for K <= 16 run on the float64 tensor-core MMA (em_sweep_dmma.cu).
+constexpr int DMMA_MAX_K = 16;
+
 int em_plan(int64_t M, int64_t N, int K, int prec, EmPlan& pl) {
   if (M <= 0 || N <= 0 || K < 1 || K > ADX_MAX_K) return ADX_ERR_ARG;
   if (prec != ADX_F64 && prec != ADX_F32 && prec != ADX_BF16 && prec != ADX_F16) return ADX_ERR_UNSUPPORTED;
@@ -422,6 +430,10 @@ int em_plan(int64_t M, int64_t N, int K, int prec, EmPlan& pl) {
   if (prec == ADX_F64) { ADX_KMAX_SWITCH(pl.kmax, CFG64) } else { ADX_KMAX_SWITCH(pl.kmax, CFG32) }
 #undef CFG64
 #undef CFG32
+  if (prec == ADX_F64 && K <= DMMA_MAX_K) {
+    W = dmma_plan_width();
+    CH = dmma_plan_chunk();
+  }
   pl.W = W; pl.CH = CH;
   pl.elem_size = prec == ADX_F64 ? sizeof(double) : sizeof(float);
   pl.n_stile = ceil_div(N, W);
@@ -485,6 +497,11 @@ int em_sweep(const EmPlan& pl, const uint8_t* G, const void* P, const void* Q, v
     void* Qb = reinterpret_cast<uint8_t*>(ws) + pl.extra_offset();
     return tc_sweep(G, (const float*)P, (const float*)Q, pl.M, pl.N, pl.K, pl.n_stile, pl.n_split,
                     pl.n_mblk, ABp, ABp + pl.ab_elems, Qb, err, pl.prec == ADX_F16, st);
+  }
+  if (pl.prec == ADX_F64 && pl.K <= DMMA_MAX_K) {
+    double* ABp = reinterpret_cast<double*>(reinterpret_cast<uint8_t*>(ws) + EmPlan::HEADER);
+    return dmma_sweep(G, (const double*)P, (const double*)Q, pl.M, pl.N, pl.K, pl.n_stile, pl.n_split,
+                      pl.n_mblk, pl.mb, ABp, ABp + pl.ab_elems, st);
   }
   return pl.prec == ADX_F64 ? launch_sweep<double>(pl, G, P, Q, ws, st)
                             : launch_sweep<float>(pl, G, P, Q, ws, st);

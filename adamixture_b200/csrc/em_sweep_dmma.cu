@@ -1,0 +1,349 @@
+// Float64 E-step sweep on the float64 tensor-core MMA (sm_100a), K <= 16.
+//
+// The same statistics as em_sweep_kernel<double> (adamixture/model/em_adam_gpu.py:46-78):
+//   h = P_j . Q_i,  rec = clamp(h, 1e-5, 1-1e-5),  a = g/rec,  b = (2-g)/(1-rec)  (0 if missing)
+//   A_j = sum_i a Q_i,  B_j = sum_i b Q_i,  T_i = sum_j (a-b) P_j + sum_j b
+// with the same partition into SNP blocks x sample splits and the same partial-sum layout
+// (AB_part[split][j][2K], T_part[snp_block][i][K], float64), so em_update_kernel<double>
+// reduces them unchanged. The CUDA-core form spends most of its issue slots folding the 2K
+// A/B values of every SNP over the warp with shuffles; here the three contractions and h
+// are float64 MMAs (mma.sync m16n8k4 .f64, 512 FMAs per warp instruction) and the CUDA
+// cores do only the per-entry ratios.
+//
+// CTA: 8 warps over a 256-sample sub-tile, 32 samples per warp, walking the block's SNPs in
+// chunks of 16 (groups of 8 chunks staged in shared memory). Per chunk a warp owns a 16-SNP
+// x 32-sample tile as four 16 x 8 MMA tiles (fragment element: SNP row g or g+8, columns
+// 2t, 2t+1; g = lane / 4, t = lane % 4). Column j of tile nt is local sample
+// 8 (j / 2) + 2 nt + (j % 2), so a thread's 8 entries per SNP row are 8 consecutive
+// samples (one 8-byte genotype load) and a pair of columns (2t, 2t+1) is a 4-sample chunk
+// of the contraction over samples:
+//   * H (16 x 8 per tile) = P_chunk (16 x K) . Q^T: ceil(K/4) k-steps of 4;
+//   * the ratios a, b per entry; a and b, read straight from the H fragments, are the A
+//     operands of A += a Q and B += b Q (16 SNPs x 8 K-columns per MMA, 4 samples per
+//     k-step; Q as the B operand);
+//   * d = a - b goes through a per-warp shared-memory transpose (samples x SNPs) to become
+//     the A operand of T += d^T P (16 samples x 8 K-columns, 4 SNPs per k-step); sum_j b
+//     is added per thread and folded over the SNP lanes at the end.
+// A and B of a chunk are summed over the 8 warps in shared memory (fixed order, double
+// buffered: one barrier per chunk) and added into the block's own AB_part rows; T lives in
+// the MMA accumulators for the whole SNP block and is written once per sub-tile.
+// Shared-memory layouts are chosen so that every fragment load and store is free of bank
+// conflicts (row strides and column swizzles below).
+#include "common.cuh"
+
+namespace adx {
+namespace dm {
+
+constexpr int WARPS = 8;
+constexpr int TPB = WARPS * 32;
+constexpr int WS = 32;                 // samples per warp
+constexpr int W = WARPS * WS;          // samples per sub-tile
+constexpr int CH = 16;                 // SNPs per chunk
+constexpr int GRP = 8;                 // chunks per staged P group
+constexpr int GS = CH * GRP;           // SNPs per group
+constexpr int QSTR = 24;               // Q tile row stride (doubles); column swizzle qsw()
+constexpr int PSTR = 20;               // P tile row stride (doubles)
+constexpr int DSTR = 20;               // transpose tile row stride (doubles); swizzle dsw()
+constexpr int NV = 16;                 // A/B accumulator values per thread (2 x 2 tiles x 4)
+
+// shared memory (doubles)
+constexpr int Q_OFF = 0;
+constexpr int P_OFF = Q_OFF + W * QSTR;
+constexpr int D_OFF = P_OFF + GS * PSTR;
+constexpr int R_OFF = D_OFF + WARPS * WS * DSTR;
+constexpr int S_OFF = R_OFF + 2 * WARPS * NV * 32;
+constexpr int SMEM_DOUBLES = S_OFF + WARPS * WS;
+constexpr size_t SMEM_BYTES = sizeof(double) * SMEM_DOUBLES;
+
+__device__ __forceinline__ int qsw(int r) { return ((r >> 3) & 3) << 2; }
+__device__ __forceinline__ int dsw(int r) { return ((r >> 3) & 3) << 2; }
+
+__device__ __forceinline__ void mma_f64(double (&d)[4], double a0, double a1, double b0) {
+  asm volatile("mma.sync.aligned.m16n8k4.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5}, {%6}, {%0,%1,%2,%3};"
+               : "+d"(d[0]), "+d"(d[1]), "+d"(d[2]), "+d"(d[3])
+               : "d"(a0), "d"(a1), "d"(b0));
+}
+
+// The genotype weight g and 2 - g (0 when missing) as doubles: the high words of 0, 1.0 and
+// 2.0 picked from a 64-bit table by the 2-bit code (low word 0).
+__device__ __forceinline__ double weight_a(uint32_t code) {
+  const uint32_t hi = (uint32_t)(0x000040003FF00000ull >> (code << 4)) << 16;
+  return __hiloint2double((int)hi, 0);
+}
+__device__ __forceinline__ double weight_b(uint32_t code) {
+  const uint32_t hi = (uint32_t)(0x000000003FF04000ull >> (code << 4)) << 16;
+  return __hiloint2double((int)hi, 0);
+}
+
+struct Args {
+  const uint8_t* G;
+  const double* P;
+  const double* Q;
+  int64_t M, N;
+  int K;
+  int64_t n_stile;
+  int n_split, n_mblk;
+  int64_t mb;
+  int vec;            // 8-byte genotype loads allowed (N % 8 == 0, G 8-byte aligned)
+  double* ABp;
+  double* Tp;
+};
+
+// KS: k-steps of 4 covering K (K <= 4 KS); NK = ceil(KS / 2) column tiles of 8.
+template <int KS>
+__global__ void __launch_bounds__(TPB, 1) em_sweep_dmma_kernel(Args a) {
+  constexpr int NK = (KS + 1) / 2;
+  extern __shared__ __align__(16) double sm[];
+  double* qt = sm + Q_OFF;   // [W][QSTR]: Q rows of the sub-tile, columns swizzled by qsw(row)
+  double* pt = sm + P_OFF;   // [GS][PSTR]: P rows of the group
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int g = lane >> 2, t = lane & 3;
+  double* dT = sm + D_OFF + warp * WS * DSTR;  // [WS][DSTR]: d^T of the warp's tile
+  double* sbuf = sm + S_OFF + warp * WS;
+  const int K = a.K;
+  const int64_t N = a.N, M = a.M;
+  const int mblk = blockIdx.x % a.n_mblk;
+  const int split = blockIdx.x / a.n_mblk;
+  const int64_t j0 = (int64_t)mblk * a.mb;
+  const int64_t j1 = min(M, j0 + a.mb);
+  const int64_t rows = (M + 3) >> 2;
+  int chunk_no = 0;   // parity of the A/B reduction buffer
+  bool first = true;
+
+  for (int64_t st = split; st < a.n_stile; st += a.n_split) {
+    const int64_t i0 = st * W;
+    // Q rows of the sub-tile (zero beyond N and K); the previous sub-tile's last reads of
+    // qt and pt came before its last chunk barrier
+    for (int e = threadIdx.x; e < W * 16; e += TPB) {
+      const int r = e >> 4, k = e & 15;
+      const int64_t i = i0 + r;
+      qt[r * QSTR + (k ^ qsw(r))] = (i < N && k < K) ? a.Q[i * K + k] : 0.0;
+    }
+    double tacc[2][NK][4];
+    double sb[4][2];
+#pragma unroll
+    for (int m = 0; m < 2; ++m)
+#pragma unroll
+      for (int n = 0; n < NK; ++n)
+#pragma unroll
+        for (int e = 0; e < 4; ++e) tacc[m][n][e] = 0.0;
+#pragma unroll
+    for (int n = 0; n < 4; ++n) sb[n][0] = sb[n][1] = 0.0;
+
+    // this thread's 8 consecutive samples
+    const int64_t s0 = i0 + warp * WS + 8 * t;
+    const bool full8 = a.vec && (s0 + 8 <= N);
+
+    for (int64_t gj = j0; gj < j1; gj += GS) {
+      const int gn = (int)min((int64_t)GS, j1 - gj);
+      for (int e = threadIdx.x; e < GS * 16; e += TPB) {
+        const int r = e >> 4, k = e & 15;
+        pt[r * PSTR + k] = (r < gn && k < K) ? a.P[(gj + r) * K + k] : 0.0;
+      }
+      __syncthreads();
+      const int nch = (gn + CH - 1) / CH;
+      for (int ch = 0; ch < nch; ++ch) {
+        const int64_t jc = gj + ch * CH;
+        const double* pc = pt + ch * CH * PSTR;
+        // genotype bytes of SNP rows g and g+8 for the thread's 8 samples
+        uint64_t w[2];
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int64_t row = min(((jc + g + 8 * h) >> 2), rows - 1);
+          const uint8_t* src = a.G + row * N + s0;
+          if (full8) {
+            w[h] = __ldg(reinterpret_cast<const unsigned long long*>(src));
+          } else {
+            uint64_t v = 0;
+#pragma unroll
+            for (int u = 0; u < 8; ++u) {
+              const uint64_t by = (s0 + u < N) ? (uint64_t)__ldg(src + u) : 0xFFull;
+              v |= by << (8 * u);
+            }
+            w[h] = v;
+          }
+          // SNPs past the block end are missing (code 3)
+          if (jc + g + 8 * h >= j1) w[h] |= 0x0303030303030303ull << (2 * (g & 3));
+          w[h] >>= 2 * (g & 3);
+        }
+        // P fragments: H's A operand (rows g, g+8; columns 4ks + t)
+        double ph[KS][2];
+#pragma unroll
+        for (int ks = 0; ks < KS; ++ks) {
+          ph[ks][0] = pc[g * PSTR + 4 * ks + t];
+          ph[ks][1] = pc[(g + 8) * PSTR + 4 * ks + t];
+        }
+        double aacc[NK][4], bacc[NK][4];
+#pragma unroll
+        for (int n = 0; n < NK; ++n)
+#pragma unroll
+          for (int e = 0; e < 4; ++e) aacc[n][e] = bacc[n][e] = 0.0;
+
+#pragma unroll
+        for (int nt = 0; nt < 4; ++nt) {
+          // H tile nt: column g of the B operand is local sample 8 (g / 2) + 2 nt + g % 2
+          const int qrow_h = warp * WS + 8 * (g >> 1) + 2 * nt + (g & 1);
+          double hacc[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+          for (int ks = 0; ks < KS; ++ks)
+            mma_f64(hacc, ph[ks][0], ph[ks][1], qt[qrow_h * QSTR + ((4 * ks + t) ^ qsw(qrow_h))]);
+          double av[4], bv[4];
+#pragma unroll
+          for (int e = 0; e < 4; ++e) {
+            // element e: SNP row g + 8 (e / 2), local sample 8t + 2nt + e % 2
+            const uint32_t code = (uint32_t)(w[e >> 1] >> (8 * (2 * nt + (e & 1)))) & 3u;
+            const double rec = fmin(fmax(hacc[e], E_CLAMP), 1.0 - E_CLAMP);
+            const double omr = 1.0 - rec;
+            // 1/rec and 1/(1-rec) from one reciprocal of x = rec (1 - rec) in [~1e-5, 0.25]:
+            // the hardware approximation refined by two Newton-Raphson steps
+            // r <- r (2 - x r), each squaring the relative error
+            const double x = rec * omr;
+            double r;
+            asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(x));
+            r = fma(r, fma(-x, r, 1.0), r);
+            r = fma(r, fma(-x, r, 1.0), r);
+            av[e] = weight_a(code) * (omr * r);
+            bv[e] = weight_b(code) * (rec * r);
+            const int srow = 8 * t + 2 * nt + (e & 1);
+            const int scol = g + 8 * (e >> 1);
+            dT[srow * DSTR + (scol ^ dsw(srow))] = av[e] - bv[e];
+          }
+          sb[nt][0] += bv[0] + bv[2];
+          sb[nt][1] += bv[1] + bv[3];
+          // A += a Q, B += b Q: k-step c of this tile is columns (2t + c): samples 8t + 2nt + c
+#pragma unroll
+          for (int c = 0; c < 2; ++c) {
+            const int qrow = warp * WS + 8 * t + 2 * nt + c;
+#pragma unroll
+            for (int n = 0; n < NK; ++n) {
+              const double qb = qt[qrow * QSTR + ((8 * n + g) ^ qsw(qrow))];
+              mma_f64(aacc[n], av[c], av[2 + c], qb);
+              mma_f64(bacc[n], bv[c], bv[2 + c], qb);
+            }
+          }
+        }
+        __syncwarp();
+        // T += d^T P: rows = local samples 16 m + g (+8), k-step q = SNPs 4q + t
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          double pb[NK];
+#pragma unroll
+          for (int n = 0; n < NK; ++n) pb[n] = pc[(4 * q + t) * PSTR + 8 * n + g];
+#pragma unroll
+          for (int m = 0; m < 2; ++m) {
+            const int r0 = 16 * m + g, r1 = r0 + 8;
+            const double d0 = dT[r0 * DSTR + ((4 * q + t) ^ dsw(r0))];
+            const double d1 = dT[r1 * DSTR + ((4 * q + t) ^ dsw(r1))];
+#pragma unroll
+            for (int n = 0; n < NK; ++n) mma_f64(tacc[m][n], d0, d1, pb[n]);
+          }
+        }
+        // A/B of the chunk: this warp's share into the reduction buffer
+        double* red = sm + R_OFF + (chunk_no & 1) * (WARPS * NV * 32);
+#pragma unroll
+        for (int n = 0; n < NK; ++n)
+#pragma unroll
+          for (int e = 0; e < 4; ++e) {
+            red[(warp * NV + n * 4 + e) * 32 + lane] = aacc[n][e];
+            red[(warp * NV + 8 + n * 4 + e) * 32 + lane] = bacc[n][e];
+          }
+        __syncthreads();
+        // sum over the warps in a fixed order; value v of lane l is (A if v < 8 else B),
+        // column tile (v / 4) % 2, element v % 4 of lane l's fragment
+        for (int e = threadIdx.x; e < NV * 32; e += TPB) {
+          const int v = e >> 5, l = e & 31;
+          const int n = (v >> 2) & 1;
+          if (n >= NK) continue;
+          const int el = v & 3;
+          const int row = (l >> 2) + 8 * (el >> 1);
+          const int col = 8 * n + 2 * (l & 3) + (el & 1);
+          const int64_t j = jc + row;
+          if (col >= K || j >= j1) continue;
+          double s = 0.0;
+#pragma unroll
+          for (int ww = 0; ww < WARPS; ++ww) s += red[(ww * NV + v) * 32 + l];
+          double* dst = a.ABp + ((int64_t)split * M + j) * (2 * K) + (v < 8 ? col : K + col);
+          *dst = first ? s : *dst + s;
+        }
+        ++chunk_no;
+      }
+      // the next group's P rows overwrite pt: every warp's T MMAs of this group are done
+      // (they precede the last chunk barrier)
+    }
+    // sum_j b over the SNP rows (lanes with the same t), then T_part = T + sum_j b
+#pragma unroll
+    for (int nt = 0; nt < 4; ++nt)
+#pragma unroll
+      for (int c = 0; c < 2; ++c) {
+        double v = sb[nt][c];
+        v += __shfl_xor_sync(0xffffffffu, v, 4);
+        v += __shfl_xor_sync(0xffffffffu, v, 8);
+        v += __shfl_xor_sync(0xffffffffu, v, 16);
+        sb[nt][c] = v;
+      }
+    if (g == 0) {
+#pragma unroll
+      for (int nt = 0; nt < 4; ++nt)
+#pragma unroll
+        for (int c = 0; c < 2; ++c) sbuf[8 * t + 2 * nt + c] = sb[nt][c];
+    }
+    __syncwarp();
+#pragma unroll
+    for (int m = 0; m < 2; ++m)
+#pragma unroll
+      for (int hh = 0; hh < 2; ++hh) {
+        const int r = 16 * m + g + 8 * hh;
+        const int64_t i = i0 + warp * WS + r;
+        if (i >= N) continue;
+        const double sbr = sbuf[r];
+        double* dst = a.Tp + ((int64_t)mblk * N + i) * K;
+#pragma unroll
+        for (int n = 0; n < NK; ++n)
+#pragma unroll
+          for (int c = 0; c < 2; ++c) {
+            const int col = 8 * n + 2 * t + c;
+            if (col < K) dst[col] = tacc[m][n][2 * hh + c] + sbr;
+          }
+      }
+    __syncwarp();
+    first = false;
+    // qt is rewritten at the next sub-tile's start: every warp's reads of it precede the
+    // last chunk barrier, which all threads have passed
+  }
+}
+
+}  // namespace dm
+
+int dmma_plan_width() { return dm::W; }
+int dmma_plan_chunk() { return dm::CH; }
+
+template <int KS>
+static int dmma_launch(const dm::Args& a, cudaStream_t st) {
+  static bool attr_set[64] = {false};
+  int dev = 0;
+  ADX_CUDA_TRY(cudaGetDevice(&dev));
+  if (dev >= 0 && dev < 64 && !attr_set[dev]) {
+    ADX_CUDA_TRY(cudaFuncSetAttribute(dm::em_sweep_dmma_kernel<KS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)dm::SMEM_BYTES));
+    attr_set[dev] = true;
+  }
+  dm::em_sweep_dmma_kernel<KS><<<(unsigned)(a.n_split * a.n_mblk), dm::TPB, dm::SMEM_BYTES, st>>>(a);
+  ADX_LAUNCH_CHECK();
+  return ADX_OK;
+}
+
+int dmma_sweep(const uint8_t* G, const double* P, const double* Q, int64_t M, int64_t N, int K,
+               int64_t n_stile, int n_split, int n_mblk, int64_t mb, double* ABp, double* Tp,
+               cudaStream_t st) {
+  if (K < 1 || K > 16) return ADX_ERR_UNSUPPORTED;
+  const int vec = ((N & 7) == 0 && (reinterpret_cast<uintptr_t>(G) & 7) == 0) ? 1 : 0;
+  const dm::Args a{G, P, Q, M, N, K, n_stile, n_split, n_mblk, mb, vec, ABp, Tp};
+  switch ((K + 3) / 4) {
+    case 1: return dmma_launch<1>(a, st);
+    case 2: return dmma_launch<2>(a, st);
+    case 3: return dmma_launch<3>(a, st);
+    default: return dmma_launch<4>(a, st);
+  }
+}
+
+}  // namespace adx

@@ -275,6 +275,8 @@ def run_reference_arm(args, cfg, rank):
 def _sweep_kernel_name(prec, K):
     if prec in TC_PRECISIONS:
         return f"em_sweep_tc_kernel<{prec == 'f16'}>"
+    if prec == "f64" and K <= 16:
+        return f"em_sweep_dmma_kernel<{(K + 3) // 4}>"
     return f"em_sweep_kernel<{'double' if prec == 'f64' else 'float'},{ops_kmax(K)}>"
 
 

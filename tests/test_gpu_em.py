@@ -138,7 +138,7 @@ def test_em_stats_f32_close_to_reference(ops, name, request):
         assert np.abs(got - ref).max() <= 2e-5 * scale
 
 
-@pytest.mark.parametrize("K", [1, 2, 3, 5, 8, 10, 13, 17, 33, 64])
+@pytest.mark.parametrize("K", [1, 2, 3, 5, 7, 8, 10, 13, 16, 17, 33, 64])
 @pytest.mark.parametrize("prec", ["f64", "f32"])
 def test_em_stats_random_shapes_vs_oracle(ops, K, prec):
     rng = np.random.default_rng(K)
@@ -168,6 +168,21 @@ def test_em_stats_large_tile_counts(ops):
     np.testing.assert_allclose(A.cpu().numpy(), A0, rtol=1e-10)
     np.testing.assert_allclose(B.cpu().numpy(), B0, rtol=1e-10)
     np.testing.assert_allclose(T.cpu().numpy(), T0, rtol=1e-10)
+
+
+def test_em_stats_f64_mma_tiles(ops):
+    # the float64 tensor-core sweep (K <= 16) with 8-byte genotype loads (N a multiple of 8),
+    # many sample sub-tiles per split, and SNP blocks that end inside a staged group
+    rng = np.random.default_rng(2)
+    for N, M, K in ((4096, 3001, 10), (2048 + 8, 517, 16), (1024, 129, 1)):
+        G = rng.integers(0, 4, size=(M, N)).astype(np.uint8)
+        P = np.clip(rng.random((M, K)), 1e-5, 1 - 1e-5)
+        Q = rng.dirichlet(np.ones(K), size=N)
+        A0, B0, T0, _ = orc.em_stats(G, P, Q)
+        A, B, T = ops.em_stats(dev_t(orc.pack(G)), dev_t(P), dev_t(Q), M, "f64")
+        for got, ref in ((A, A0), (B, B0), (T, T0)):
+            err = np.abs(got.cpu().numpy() - ref).max() / np.abs(ref).max()
+            assert err <= 1e-12, (N, M, K, err)
 
 
 # ------------------------------------------------------------------ iterations
