@@ -471,12 +471,9 @@ static int launch_sweep(const EmPlan& pl, const uint8_t* G, const void* P, const
 }
 
 template <typename R>
-static int launch_update(const EmPlan& pl, void* ws, int mode, double* A, double* B, double* T,
-                         const double* q_bat, double* P, double* Q, float* P32, float* Q32,
-                         double* mP, double* vP, double* mQ, double* vQ, AdamArgs ad,
-                         cudaStream_t st) {
-  const R* ABp = reinterpret_cast<const R*>(reinterpret_cast<const uint8_t*>(ws) + EmPlan::HEADER);
-  const R* Tp = ABp + pl.ab_elems;
+static int launch_update_from(const EmPlan& pl, const R* ABp, const R* Tp, int mode, double* A, double* B,
+                              double* T, const double* q_bat, double* P, double* Q, float* P32, float* Q32,
+                              double* mP, double* vP, double* mQ, double* vQ, AdamArgs ad, cudaStream_t st) {
   const int threads = 128;
   const dim3 grid((unsigned)ceil_div(pl.M + pl.N, threads));
 #define LAUNCH(KM)                                                                          \
@@ -487,6 +484,16 @@ static int launch_update(const EmPlan& pl, void* ws, int mode, double* A, double
 #undef LAUNCH
   ADX_LAUNCH_CHECK();
   return ADX_OK;
+}
+
+template <typename R>
+static int launch_update(const EmPlan& pl, void* ws, int mode, double* A, double* B, double* T,
+                         const double* q_bat, double* P, double* Q, float* P32, float* Q32,
+                         double* mP, double* vP, double* mQ, double* vQ, AdamArgs ad,
+                         cudaStream_t st) {
+  const R* ABp = reinterpret_cast<const R*>(reinterpret_cast<const uint8_t*>(ws) + EmPlan::HEADER);
+  return launch_update_from<R>(pl, ABp, ABp + pl.ab_elems, mode, A, B, T, q_bat, P, Q, P32, Q32, mP, vP, mQ,
+                               vQ, ad, st);
 }
 
 int em_sweep(const EmPlan& pl, const uint8_t* G, const void* P, const void* Q, void* ws,
@@ -674,4 +681,92 @@ extern "C" int adx_em_adam_iteration(const uint8_t* G, int64_t M, int64_t N, int
   if (rc) return rc;
   return em_update(pl, workspace, 1, nullptr, nullptr, nullptr, q_bat, P, Q, P32, Q32, mP, vP, mQ,
                    vQ, AdamArgs{t, lr, beta1, beta2, eps}, st);
+}
+
+// ---------------------------------------------------------------- batched float64 E-step
+//
+// Several E-step problems on one cohort (K <= 16 each; e.g. the K sweep and its cross-
+// validation folds) in one launch of the float64 tensor-core sweep. All of them share the
+// float64 sweep's partition (it does not depend on K), so each problem's partial sums, and
+// hence its statistics, are bit-identical to a single-problem sweep of the same P, Q and
+// (fold-masked) genotypes. Workspace: a 256-byte header, then per problem its A/B partials
+// and T partials, each 256-byte aligned.
+
+namespace adx {
+int dmma_sweep_batch(const uint8_t* G, int64_t M, int64_t N, int n, const int* K, const int* fold,
+                     const double* const* P, const double* const* Q, double* const* ABp, double* const* Tp,
+                     uint64_t seed, int n_buckets, int64_t n_stile, int n_split, int n_mblk, int64_t mb,
+                     cudaStream_t st);
+}
+
+static int batch_layout(int64_t M, int64_t N, int n, const int* K, EmPlan& pl, size_t* offs, size_t* total) {
+  if (n < 1 || n > 64 || !K) return ADX_ERR_ARG;
+  for (int p = 0; p < n; ++p)
+    if (K[p] < 1 || K[p] > DMMA_MAX_K) return ADX_ERR_ARG;
+  const int rc = em_plan(M, N, K[0], ADX_F64, pl);
+  if (rc) return rc;
+  size_t off = EmPlan::HEADER;
+  for (int p = 0; p < n; ++p) {
+    if (offs) offs[p] = off;
+    const size_t ab = (size_t)pl.n_split * (size_t)M * 2 * K[p], tt = (size_t)pl.n_mblk * (size_t)N * K[p];
+    off = (off + (ab + tt) * sizeof(double) + 255) & ~size_t(255);
+  }
+  *total = off;
+  return ADX_OK;
+}
+
+extern "C" int adx_em_batch_workspace_bytes(int64_t M, int64_t N, int n, const int* K, size_t* bytes) {
+  EmPlan pl;
+  if (!bytes) return ADX_ERR_ARG;
+  const int rc = batch_layout(M, N, n, K, pl, nullptr, bytes);
+  if (rc) adx_set_message("adx_em_batch_workspace_bytes: bad shape or K (1 <= n <= 64 problems, 1 <= K <= 16)");
+  return rc;
+}
+
+extern "C" int adx_em_sweep_batch(const uint8_t* G, int64_t M, int64_t N, int n, const int* K, const int* fold,
+                                  uint64_t seed, int n_buckets, const double* const* P, const double* const* Q,
+                                  void* workspace, size_t workspace_bytes, void* stream) {
+  EmPlan pl;
+  size_t offs[64], total = 0;
+  int rc = batch_layout(M, N, n, K, pl, offs, &total);
+  if (rc || !G || !fold || !P || !Q || !workspace || n_buckets < 1) {
+    adx_set_message("adx_em_sweep_batch: bad argument (1 <= n <= 64 problems, 1 <= K <= 16, n_buckets >= 1)");
+    return rc ? rc : ADX_ERR_ARG;
+  }
+  if (workspace_bytes < total) { adx_set_message("adx_em_sweep_batch: workspace too small"); return ADX_ERR_WORKSPACE; }
+  double* ABp[64];
+  double* Tp[64];
+  for (int p = 0; p < n; ++p) {
+    if (!P[p] || !Q[p] || fold[p] >= n_buckets) { adx_set_message("adx_em_sweep_batch: bad problem"); return ADX_ERR_ARG; }
+    ABp[p] = reinterpret_cast<double*>(static_cast<uint8_t*>(workspace) + offs[p]);
+    Tp[p] = ABp[p] + (size_t)pl.n_split * (size_t)M * 2 * K[p];
+  }
+  rc = dmma_sweep_batch(G, M, N, n, K, fold, P, Q, ABp, Tp, seed, n_buckets, pl.n_stile, pl.n_split, pl.n_mblk,
+                        pl.mb, as_stream(stream));
+  if (rc == ADX_ERR_ARG) adx_set_message("adx_em_sweep_batch: bad problem");
+  return rc;
+}
+
+extern "C" int adx_em_batch_apply(int64_t M, int64_t N, int n, const int* K, int p, int mode, double* A, double* B,
+                                  double* T, const double* q_bat, double* P, double* Q, double* mP, double* vP,
+                                  double* mQ, double* vQ, double t, double lr, double beta1, double beta2,
+                                  double eps, void* workspace, size_t workspace_bytes, void* stream) {
+  EmPlan pl;
+  size_t offs[64], total = 0;
+  const int rc = batch_layout(M, N, n, K, pl, offs, &total);
+  if (rc || p < 0 || p >= n || !workspace || (mode != 0 && mode != 1)) {
+    adx_set_message("adx_em_batch_apply: bad argument");
+    return rc ? rc : ADX_ERR_ARG;
+  }
+  if (workspace_bytes < total) { adx_set_message("adx_em_batch_apply: workspace too small"); return ADX_ERR_WORKSPACE; }
+  if (mode == 0 ? (!A || !B || !T) : (!q_bat || !P || !Q || !mP || !vP || !mQ || !vQ || t < 1)) {
+    adx_set_message("adx_em_batch_apply: bad argument");
+    return ADX_ERR_ARG;
+  }
+  EmPlan pp;
+  em_plan(M, N, K[p], ADX_F64, pp);
+  const double* ABp = reinterpret_cast<const double*>(static_cast<const uint8_t*>(workspace) + offs[p]);
+  const double* Tp = ABp + (size_t)pl.n_split * (size_t)M * 2 * K[p];
+  return launch_update_from<double>(pp, ABp, Tp, mode, A, B, T, q_bat, P, Q, nullptr, nullptr, mP, vP, mQ, vQ,
+                                    AdamArgs{t, lr, beta1, beta2, eps}, as_stream(stream));
 }

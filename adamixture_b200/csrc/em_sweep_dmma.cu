@@ -75,23 +75,77 @@ __device__ __forceinline__ double weight_b(uint32_t code) {
   return __hiloint2double((int)hi, 0);
 }
 
+// The genotype bytes of SNP rows g and g+8 of the chunk at jc for the thread's 8 samples
+// from s0 (0xFF, all missing, past N); rows past the matrix read its last row (those SNPs
+// are masked as missing by the caller).
+__device__ __forceinline__ void load_words(const uint8_t* __restrict__ G, int64_t N, int64_t rows, int64_t jc,
+                                           int g, int64_t s0, bool full8, uint64_t (&w)[2]) {
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    const int64_t row = min(((jc + g + 8 * h) >> 2), rows - 1);
+    const uint8_t* src = G + row * N + s0;
+    if (full8) {
+      w[h] = __ldg(reinterpret_cast<const unsigned long long*>(src));
+    } else {
+      uint64_t v = 0;
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
+        const uint64_t by = (s0 + u < N) ? (uint64_t)__ldg(src + u) : 0xFFull;
+        v |= by << (8 * u);
+      }
+      w[h] = v;
+    }
+  }
+}
+
 struct Args {
   const uint8_t* G;
-  const double* P;
-  const double* Q;
   int64_t M, N;
-  int K;
   int64_t n_stile;
   int n_split, n_mblk;
   int64_t mb;
   int vec;            // 8-byte genotype loads allowed (N % 8 == 0, G 8-byte aligned)
-  double* ABp;
-  double* Tp;
+  uint64_t seed;      // fold rule: entry j*N + i is held out of a problem with fold f when
+  int n_buckets;      //   fold_hash(j*N + i, seed) % n_buckets == f
 };
 
-// KS: k-steps of 4 covering K (K <= 4 KS); NK = ceil(KS / 2) column tiles of 8.
-template <int KS>
-__global__ void __launch_bounds__(TPB, 1) em_sweep_dmma_kernel(Args a) {
+// One E-step problem: its P [M][K] and Q [N][K] (float64), its partial sums, and the fold
+// whose entries it treats as missing (-1: none).
+struct Prob {
+  const double* P;
+  const double* Q;
+  double* ABp;
+  double* Tp;
+  int K;
+  int fold;
+};
+
+template <int MAXP>
+struct Probs {
+  Prob p[MAXP];
+  int n;
+};
+
+// The cross-validation hash of a flat index j*N + i (the reference's rule,
+// adamixture/src/cv.py:58-78; identical to cv::fold_hash).
+__device__ __forceinline__ uint64_t fold_hash_dm(uint64_t flat, uint64_t seed) {
+  uint64_t h = flat + seed + 0x9E3779B97F4A7C15ull;
+  h ^= h >> 30;
+  h *= 0xBF58476D1CE4E5B9ull;
+  h ^= h >> 27;
+  h *= 0x94D049BB133111EBull;
+  h ^= h >> 31;
+  return h;
+}
+
+// KS: k-steps of 4 covering every problem's K (K <= 4 KS); NK = ceil(KS / 2) column tiles
+// of 8. NB: the fold rule's bucket count as a constant (0: taken from the arguments). A
+// CTA runs, for each of its sample sub-tiles, every problem in turn over its SNP block, so
+// the block's genotype tile is read from memory once and served from cache to the others;
+// a problem's arithmetic and summation order do not depend on the other problems, on KS
+// beyond its own K, or on NB.
+template <int KS, int NB, int MAXP>
+__global__ void __launch_bounds__(TPB, 1) em_sweep_dmma_kernel(Args a, Probs<MAXP> ps) {
   constexpr int NK = (KS + 1) / 2;
   extern __shared__ __align__(16) double sm[];
   double* qt = sm + Q_OFF;   // [W][QSTR]: Q rows of the sub-tile, columns swizzled by qsw(row)
@@ -100,7 +154,6 @@ __global__ void __launch_bounds__(TPB, 1) em_sweep_dmma_kernel(Args a) {
   const int g = lane >> 2, t = lane & 3;
   double* dT = sm + D_OFF + warp * WS * DSTR;  // [WS][DSTR]: d^T of the warp's tile
   double* sbuf = sm + S_OFF + warp * WS;
-  const int K = a.K;
   const int64_t N = a.N, M = a.M;
   const int mblk = blockIdx.x % a.n_mblk;
   const int split = blockIdx.x / a.n_mblk;
@@ -108,16 +161,19 @@ __global__ void __launch_bounds__(TPB, 1) em_sweep_dmma_kernel(Args a) {
   const int64_t j1 = min(M, j0 + a.mb);
   const int64_t rows = (M + 3) >> 2;
   int chunk_no = 0;   // parity of the A/B reduction buffer
-  bool first = true;
 
-  for (int64_t st = split; st < a.n_stile; st += a.n_split) {
+  for (int64_t st = split; st < a.n_stile; st += a.n_split)
+  for (int pi = 0; pi < (MAXP == 1 ? 1 : ps.n); ++pi) {
+    const Prob pr = ps.p[pi];
+    const int K = pr.K;
+    const bool first = st == split;   // this CTA's first sub-tile: AB_part rows are written
     const int64_t i0 = st * W;
     // Q rows of the sub-tile (zero beyond N and K); the previous sub-tile's last reads of
     // qt and pt came before its last chunk barrier
     for (int e = threadIdx.x; e < W * 16; e += TPB) {
       const int r = e >> 4, k = e & 15;
       const int64_t i = i0 + r;
-      qt[r * QSTR + (k ^ qsw(r))] = (i < N && k < K) ? a.Q[i * K + k] : 0.0;
+      qt[r * QSTR + (k ^ qsw(r))] = (i < N && k < K) ? pr.Q[i * K + k] : 0.0;
     }
     double tacc[2][NK][4];
     double sb[4][2];
@@ -130,41 +186,55 @@ __global__ void __launch_bounds__(TPB, 1) em_sweep_dmma_kernel(Args a) {
 #pragma unroll
     for (int n = 0; n < 4; ++n) sb[n][0] = sb[n][1] = 0.0;
 
-    // this thread's 8 consecutive samples
+    // this thread's 8 consecutive samples; the first chunk's genotype words are loaded
+    // here and each chunk loads the next one's, a chunk ahead of their use
     const int64_t s0 = i0 + warp * WS + 8 * t;
     const bool full8 = a.vec && (s0 + 8 <= N);
+    uint64_t wnext[2];
+    load_words(a.G, N, rows, j0, g, s0, full8, wnext);
 
     for (int64_t gj = j0; gj < j1; gj += GS) {
       const int gn = (int)min((int64_t)GS, j1 - gj);
       for (int e = threadIdx.x; e < GS * 16; e += TPB) {
         const int r = e >> 4, k = e & 15;
-        pt[r * PSTR + k] = (r < gn && k < K) ? a.P[(gj + r) * K + k] : 0.0;
+        pt[r * PSTR + k] = (r < gn && k < K) ? pr.P[(gj + r) * K + k] : 0.0;
       }
       __syncthreads();
       const int nch = (gn + CH - 1) / CH;
       for (int ch = 0; ch < nch; ++ch) {
         const int64_t jc = gj + ch * CH;
         const double* pc = pt + ch * CH * PSTR;
-        // genotype bytes of SNP rows g and g+8 for the thread's 8 samples
-        uint64_t w[2];
+        uint64_t w[2] = {wnext[0], wnext[1]};
+        if (jc + CH < j1) load_words(a.G, N, rows, jc + CH, g, s0, full8, wnext);
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
-          const int64_t row = min(((jc + g + 8 * h) >> 2), rows - 1);
-          const uint8_t* src = a.G + row * N + s0;
-          if (full8) {
-            w[h] = __ldg(reinterpret_cast<const unsigned long long*>(src));
-          } else {
-            uint64_t v = 0;
-#pragma unroll
-            for (int u = 0; u < 8; ++u) {
-              const uint64_t by = (s0 + u < N) ? (uint64_t)__ldg(src + u) : 0xFFull;
-              v |= by << (8 * u);
-            }
-            w[h] = v;
-          }
           // SNPs past the block end are missing (code 3)
           if (jc + g + 8 * h >= j1) w[h] |= 0x0303030303030303ull << (2 * (g & 3));
           w[h] >>= 2 * (g & 3);
+          // the problem's held-out entries are missing too
+          if (pr.fold >= 0) {
+            const uint64_t flat0 = (uint64_t)(jc + g + 8 * h) * (uint64_t)N + (uint64_t)s0;
+#pragma unroll
+            for (int u = 0; u < 8; ++u) {
+              const uint64_t hv = fold_hash_dm(flat0 + u, a.seed);
+              const uint64_t b = NB > 0 ? hv % (uint64_t)NB : hv % (uint64_t)a.n_buckets;
+              if (b == (uint64_t)pr.fold) w[h] |= 3ull << (8 * u);
+            }
+          }
+        }
+        // this thread's two A/B partial sums of the chunk, read now so that the read's
+        // latency overlaps the chunk's arithmetic (added after the chunk barrier)
+        double old_ab[2] = {0.0, 0.0};
+        if (!first) {
+#pragma unroll
+          for (int u = 0; u < 2; ++u) {
+            const int e = threadIdx.x + u * TPB;
+            const int v = e >> 5, l = e & 31, n = (v >> 2) & 1, el = v & 3;
+            const int row = (l >> 2) + 8 * (el >> 1);
+            const int col = 8 * n + 2 * (l & 3) + (el & 1);
+            if (n < NK && col < K && jc + row < j1)
+              old_ab[u] = pr.ABp[((int64_t)split * M + jc + row) * (2 * K) + (v < 8 ? col : K + col)];
+          }
         }
         // P fragments: H's A operand (rows g, g+8; columns 4ks + t)
         double ph[KS][2];
@@ -179,14 +249,25 @@ __global__ void __launch_bounds__(TPB, 1) em_sweep_dmma_kernel(Args a) {
 #pragma unroll
           for (int e = 0; e < 4; ++e) aacc[n][e] = bacc[n][e] = 0.0;
 
-#pragma unroll
-        for (int nt = 0; nt < 4; ++nt) {
-          // H tile nt: column g of the B operand is local sample 8 (g / 2) + 2 nt + g % 2
-          const int qrow_h = warp * WS + 8 * (g >> 1) + 2 * nt + (g & 1);
-          double hacc[4] = {0.0, 0.0, 0.0, 0.0};
+        // H of tile nt + 1 is issued before tile nt's ratios, so the MMAs' latency overlaps them
+        double hcur[4] = {0.0, 0.0, 0.0, 0.0}, hnext[4];
+        {
+          const int qrow_h = warp * WS + 8 * (g >> 1) + (g & 1);
 #pragma unroll
           for (int ks = 0; ks < KS; ++ks)
-            mma_f64(hacc, ph[ks][0], ph[ks][1], qt[qrow_h * QSTR + ((4 * ks + t) ^ qsw(qrow_h))]);
+            mma_f64(hcur, ph[ks][0], ph[ks][1], qt[qrow_h * QSTR + ((4 * ks + t) ^ qsw(qrow_h))]);
+        }
+#pragma unroll
+        for (int nt = 0; nt < 4; ++nt) {
+          if (nt < 3) {
+            // H tile nt+1: column g of the B operand is local sample 8 (g / 2) + 2 (nt+1) + g % 2
+            const int qrow_h = warp * WS + 8 * (g >> 1) + 2 * (nt + 1) + (g & 1);
+            hnext[0] = hnext[1] = hnext[2] = hnext[3] = 0.0;
+#pragma unroll
+            for (int ks = 0; ks < KS; ++ks)
+              mma_f64(hnext, ph[ks][0], ph[ks][1], qt[qrow_h * QSTR + ((4 * ks + t) ^ qsw(qrow_h))]);
+          }
+          const double (&hacc)[4] = hcur;
           double av[4], bv[4];
 #pragma unroll
           for (int e = 0; e < 4; ++e) {
@@ -221,6 +302,10 @@ __global__ void __launch_bounds__(TPB, 1) em_sweep_dmma_kernel(Args a) {
               mma_f64(bacc[n], bv[c], bv[2 + c], qb);
             }
           }
+          if (nt < 3) {
+#pragma unroll
+            for (int e = 0; e < 4; ++e) hcur[e] = hnext[e];
+          }
         }
         __syncwarp();
         // T += d^T P: rows = local samples 16 m + g (+8), k-step q = SNPs 4q + t
@@ -250,7 +335,9 @@ __global__ void __launch_bounds__(TPB, 1) em_sweep_dmma_kernel(Args a) {
         __syncthreads();
         // sum over the warps in a fixed order; value v of lane l is (A if v < 8 else B),
         // column tile (v / 4) % 2, element v % 4 of lane l's fragment
-        for (int e = threadIdx.x; e < NV * 32; e += TPB) {
+#pragma unroll
+        for (int u = 0; u < 2; ++u) {
+          const int e = threadIdx.x + u * TPB;
           const int v = e >> 5, l = e & 31;
           const int n = (v >> 2) & 1;
           if (n >= NK) continue;
@@ -262,8 +349,8 @@ __global__ void __launch_bounds__(TPB, 1) em_sweep_dmma_kernel(Args a) {
           double s = 0.0;
 #pragma unroll
           for (int ww = 0; ww < WARPS; ++ww) s += red[(ww * NV + v) * 32 + l];
-          double* dst = a.ABp + ((int64_t)split * M + j) * (2 * K) + (v < 8 ? col : K + col);
-          *dst = first ? s : *dst + s;
+          double* dst = pr.ABp + ((int64_t)split * M + j) * (2 * K) + (v < 8 ? col : K + col);
+          *dst = first ? s : old_ab[u] + s;
         }
         ++chunk_no;
       }
@@ -296,7 +383,7 @@ __global__ void __launch_bounds__(TPB, 1) em_sweep_dmma_kernel(Args a) {
         const int64_t i = i0 + warp * WS + r;
         if (i >= N) continue;
         const double sbr = sbuf[r];
-        double* dst = a.Tp + ((int64_t)mblk * N + i) * K;
+        double* dst = pr.Tp + ((int64_t)mblk * N + i) * K;
 #pragma unroll
         for (int n = 0; n < NK; ++n)
 #pragma unroll
@@ -306,8 +393,7 @@ __global__ void __launch_bounds__(TPB, 1) em_sweep_dmma_kernel(Args a) {
           }
       }
     __syncwarp();
-    first = false;
-    // qt is rewritten at the next sub-tile's start: every warp's reads of it precede the
+    // qt is rewritten at the next (sub-tile, problem)'s start: every warp's reads of it precede the
     // last chunk barrier, which all threads have passed
   }
 }
@@ -317,33 +403,66 @@ __global__ void __launch_bounds__(TPB, 1) em_sweep_dmma_kernel(Args a) {
 int dmma_plan_width() { return dm::W; }
 int dmma_plan_chunk() { return dm::CH; }
 
-template <int KS>
-static int dmma_launch(const dm::Args& a, cudaStream_t st) {
+template <int KS, int NB, int MAXP>
+static int dmma_launch(const dm::Args& a, const dm::Probs<MAXP>& ps, cudaStream_t st) {
   static bool attr_set[64] = {false};
   int dev = 0;
   ADX_CUDA_TRY(cudaGetDevice(&dev));
   if (dev >= 0 && dev < 64 && !attr_set[dev]) {
-    ADX_CUDA_TRY(cudaFuncSetAttribute(dm::em_sweep_dmma_kernel<KS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)dm::SMEM_BYTES));
+    ADX_CUDA_TRY(cudaFuncSetAttribute(dm::em_sweep_dmma_kernel<KS, NB, MAXP>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dm::SMEM_BYTES));
     attr_set[dev] = true;
   }
-  dm::em_sweep_dmma_kernel<KS><<<(unsigned)(a.n_split * a.n_mblk), dm::TPB, dm::SMEM_BYTES, st>>>(a);
+  dm::em_sweep_dmma_kernel<KS, NB, MAXP><<<(unsigned)(a.n_split * a.n_mblk), dm::TPB, dm::SMEM_BYTES, st>>>(a, ps);
   ADX_LAUNCH_CHECK();
   return ADX_OK;
+}
+
+static int dmma_vec(const uint8_t* G, int64_t N) {
+  return ((N & 7) == 0 && (reinterpret_cast<uintptr_t>(G) & 7) == 0) ? 1 : 0;
 }
 
 int dmma_sweep(const uint8_t* G, const double* P, const double* Q, int64_t M, int64_t N, int K,
                int64_t n_stile, int n_split, int n_mblk, int64_t mb, double* ABp, double* Tp,
                cudaStream_t st) {
   if (K < 1 || K > 16) return ADX_ERR_UNSUPPORTED;
-  const int vec = ((N & 7) == 0 && (reinterpret_cast<uintptr_t>(G) & 7) == 0) ? 1 : 0;
-  const dm::Args a{G, P, Q, M, N, K, n_stile, n_split, n_mblk, mb, vec, ABp, Tp};
+  const dm::Args a{G, M, N, n_stile, n_split, n_mblk, mb, dmma_vec(G, N), 0, 0};
+  dm::Probs<1> ps;
+  ps.p[0] = dm::Prob{P, Q, ABp, Tp, K, -1};
+  ps.n = 1;
   switch ((K + 3) / 4) {
-    case 1: return dmma_launch<1>(a, st);
-    case 2: return dmma_launch<2>(a, st);
-    case 3: return dmma_launch<3>(a, st);
-    default: return dmma_launch<4>(a, st);
+    case 1: return dmma_launch<1, 0, 1>(a, ps, st);
+    case 2: return dmma_launch<2, 0, 1>(a, ps, st);
+    case 3: return dmma_launch<3, 0, 1>(a, ps, st);
+    default: return dmma_launch<4, 0, 1>(a, ps, st);
   }
+}
+
+constexpr int DMMA_MAX_PROBLEMS = 64;
+
+int dmma_sweep_batch(const uint8_t* G, int64_t M, int64_t N, int n, const int* K, const int* fold,
+                     const double* const* P, const double* const* Q, double* const* ABp, double* const* Tp,
+                     uint64_t seed, int n_buckets, int64_t n_stile, int n_split, int n_mblk, int64_t mb,
+                     cudaStream_t st) {
+  if (n < 1 || n > DMMA_MAX_PROBLEMS || n_buckets < 1) return ADX_ERR_ARG;
+  const dm::Args a{G, M, N, n_stile, n_split, n_mblk, mb, dmma_vec(G, N), seed, n_buckets};
+  dm::Probs<DMMA_MAX_PROBLEMS> ps;
+  int kmax = 1;
+  for (int p = 0; p < n; ++p) {
+    if (K[p] < 1 || K[p] > 16 || fold[p] >= n_buckets) return ADX_ERR_ARG;
+    ps.p[p] = dm::Prob{P[p], Q[p], ABp[p], Tp[p], K[p], fold[p] < 0 ? -1 : fold[p]};
+    kmax = K[p] > kmax ? K[p] : kmax;
+  }
+  ps.n = n;
+  const bool ten = n_buckets == 10;
+#define ADX_DM_BATCH(KS) return ten ? dmma_launch<KS, 10, DMMA_MAX_PROBLEMS>(a, ps, st) : dmma_launch<KS, 0, DMMA_MAX_PROBLEMS>(a, ps, st)
+  switch ((kmax + 3) / 4) {
+    case 1: ADX_DM_BATCH(1);
+    case 2: ADX_DM_BATCH(2);
+    case 3: ADX_DM_BATCH(3);
+    default: ADX_DM_BATCH(4);
+  }
+#undef ADX_DM_BATCH
 }
 
 }  // namespace adx

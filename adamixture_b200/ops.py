@@ -239,6 +239,64 @@ def em_adam_iteration(G, P, Q, P32, Q32, mP, vP, mQ, vQ, q_bat, M, t, lr, beta1,
          ws.data_ptr(), ws.numel(), _stream(dev))
 
 
+# ---------------------------------------------------------------- batched float64 E-step
+
+class EmBatch:
+    """Host-side description of a batch of float64 E-step problems on one cohort (the
+    C arrays the batch entry points take) and its partial-sum workspace."""
+
+    def __init__(self, M: int, N: int, Ks, folds, seed: int = 0, n_buckets: int = 10, device=None):
+        import ctypes
+
+        self.M, self.N = int(M), int(N)
+        self.n = len(Ks)
+        self.K = (ctypes.c_int * self.n)(*[int(k) for k in Ks])
+        self.fold = (ctypes.c_int * self.n)(*[int(f) for f in folds])
+        self.seed, self.n_buckets = int(seed), int(n_buckets)
+        nbytes = query_size("adx_em_batch_workspace_bytes", self.M, self.N, self.n, ctypes.addressof(self.K))
+        dev = torch.device("cuda", torch.cuda.current_device()) if device is None else torch.device(device)
+        self.workspace = Workspace.get(dev, nbytes, tag="em_batch")
+
+    def sweep(self, G: torch.Tensor, Ps, Qs) -> None:
+        """One batched sweep over the problems (P, Q: float64 device tensors)."""
+        import ctypes
+
+        _check(G, "G", torch.uint8)
+        for P, Q, k in zip(Ps, Qs, self.K):
+            _check(P, "P", torch.float64, G.device)
+            _check(Q, "Q", torch.float64, G.device)
+            if P.shape != (self.M, k) or Q.shape != (self.N, k):
+                raise ValueError("P/Q shapes do not match the batch")
+        pp = (ctypes.c_void_p * self.n)(*[P.data_ptr() for P in Ps])
+        qq = (ctypes.c_void_p * self.n)(*[Q.data_ptr() for Q in Qs])
+        call("adx_em_sweep_batch", G.data_ptr(), self.M, self.N, self.n, ctypes.addressof(self.K),
+             ctypes.addressof(self.fold), self.seed, self.n_buckets, ctypes.addressof(pp), ctypes.addressof(qq),
+             self.workspace.data_ptr(), self.workspace.numel(), _stream(G.device))
+
+    def stats(self, p: int):
+        """A, B, T of problem p from the last sweep."""
+        import ctypes
+
+        dev = self.workspace.device
+        K = self.K[p]
+        A = torch.empty((self.M, K), dtype=torch.float64, device=dev)
+        B = torch.empty_like(A)
+        T = torch.empty((self.N, K), dtype=torch.float64, device=dev)
+        call("adx_em_batch_apply", self.M, self.N, self.n, ctypes.addressof(self.K), p, 0, A.data_ptr(),
+             B.data_ptr(), T.data_ptr(), None, None, None, None, None, None, None, 1.0, 0.0, 0.0, 0.0, 0.0,
+             self.workspace.data_ptr(), self.workspace.numel(), _stream(dev))
+        return A, B, T
+
+    def adam(self, p: int, P, Q, mP, vP, mQ, vQ, q_bat, t, lr, beta1, beta2, eps) -> None:
+        """EM targets and the Adam move of problem p from the last sweep, in place."""
+        import ctypes
+
+        call("adx_em_batch_apply", self.M, self.N, self.n, ctypes.addressof(self.K), p, 1, None, None, None,
+             q_bat.data_ptr(), P.data_ptr(), Q.data_ptr(), mP.data_ptr(), vP.data_ptr(), mQ.data_ptr(),
+             vQ.data_ptr(), float(t), float(lr), float(beta1), float(beta2), float(eps),
+             self.workspace.data_ptr(), self.workspace.numel(), _stream(P.device))
+
+
 def loglik_device(G: torch.Tensor, P: torch.Tensor, Q: torch.Tensor, M: int, precision="f64",
                   out: torch.Tensor | None = None) -> torch.Tensor:
     """Log-likelihood as a device float64 scalar (no host sync)."""

@@ -58,6 +58,8 @@ CONFIGS = {
                N=10_000, M=200_000, K=8, F=0.05, alpha=0.3, miss=0.005, seed=1000),
     "c1": dict(workload="Adam-EM, N=1000 samples, M=10000 SNPs, K=3, F=0.1, Q Dir(0.5), 1% missing",
                N=1_000, M=10_000, K=3, F=0.1, alpha=0.5, miss=0.01, seed=0),
+    "c4": dict(workload="K sweep K=2..12 with 5-fold CV (10 % of entries per fold, seeded hash), N=20000 samples, M=100000 SNPs, true K=6, F=0.08, Q Dir(0.5), 1% missing",
+               N=20_000, M=100_000, K=6, F=0.08, alpha=0.5, miss=0.01, seed=4000),
     # the c3 cohort's generator at one tenth of its SNPs (2.5 GB packed): the size profiled
     # under ncu, whose full capture saves and restores device memory on every pass
     "c3s": dict(workload="Adam-EM, N=200000 samples, M=50000 SNPs, K=10, F=0.02, Q 0.7*Dir(0.05)+0.3*Dir(1), 1% missing",
@@ -853,6 +855,58 @@ def run_errors(args, cfg):
         "loglik": "float64 log-likelihood of each run's own P, Q"}, "runs": out}), flush=True)
 
 
+def run_cv_batch(args, cfg):
+    """``--config c4``: the K sweep K=2..12 and 5-fold cross-validation (10 % of the
+    entries per fold by the seeded hash rule) as batched problems -- every iteration one
+    launch of the batched float64 sweep over all live problems -- against the same problems
+    run one at a time through the single-problem path. Reports both wall times, the largest
+    difference between their P/Q, and the CV index per K. One JSON line."""
+    import torch
+
+    from adamixture_b200 import ops
+    from adamixture_b200.model.em_adam_batch import cross_validate
+    from adamixture_b200.src.simulate import make_cohort
+
+    dev = torch.device("cuda", 0)
+    N, M = cfg["N"], cfg["M"]
+    coh = make_cohort(N, M, cfg["K"], cfg["F"], cfg["alpha"], cfg["miss"], cfg["seed"])
+    G = ops.simulate_packed(torch.from_numpy(coh.Pq.astype(np.int32)).to(dev),
+                            torch.from_numpy(coh.Qq.astype(np.int32)).to(dev), coh.miss_q, coh.keys)
+    Ks = list(range(2, 13))
+    starts = {}
+    for K in Ks:
+        rng = np.random.default_rng(cfg["seed"] + K)
+        P0 = np.clip(rng.random((M, K)), 1e-5, 1 - 1e-5)
+        Q0 = np.clip(rng.random((N, K)), 1e-5, 1 - 1e-5)
+        Q0 /= Q0.sum(1, keepdims=True)
+        starts[K] = (torch.from_numpy(P0).to(dev), torch.from_numpy(Q0).to(dev))
+    kw = dict(n_folds=5, n_buckets=10, seed=42, polish_iters=args.cv_polish, max_iter=args.cv_max_iter)
+    # load the kernel instances both paths use before timing
+    cross_validate(G, M, N, [2, 12], starts, **{**kw, "max_iter": 5, "polish_iters": 1}, batched=True)
+    cross_validate(G, M, N, [2, 12], starts, **{**kw, "max_iter": 5, "polish_iters": 1}, batched=False)
+    b = cross_validate(G, M, N, Ks, starts, batched=True, **kw)
+    s = cross_validate(G, M, N, Ks, starts, batched=False, **kw)
+    dmax = 0.0
+    for K in Ks:
+        for x, y in zip(b["fits"][K], s["fits"][K]):
+            dmax = max(dmax, float((x - y).abs().max()))
+        for f in range(5):
+            for x, y in zip(b["folds"][(K, f)], s["folds"][(K, f)]):
+                dmax = max(dmax, float((x - y).abs().max()))
+    cv_rel = max(abs(b["cv"][K] - s["cv"][K]) / abs(s["cv"][K]) for K in Ks)
+    line = {"metric": "K sweep + cross-validation, batched vs one problem at a time",
+            "config": {"workload": cfg["workload"], "Ks": Ks, "folds": 5, "fold_rule": "reference hash, 10 buckets, "
+                       "folds 0..4", "polish_iters": args.cv_polish, "max_iter": args.cv_max_iter,
+                       "arithmetic": "float64 (tensor-core MMA sweep)"},
+            "batched_seconds": b["seconds"], "sequential_seconds": s["seconds"],
+            "speedup": (s["seconds"]["fits"] + s["seconds"]["folds"]) / (b["seconds"]["fits"] + b["seconds"]["folds"]),
+            "max_abs_diff_PQ": dmax, "max_rel_diff_cv": cv_rel,
+            "cv_index": {str(K): b["cv"][K] for K in Ks}, "best_K": min(b["cv"], key=b["cv"].get),
+            "held_out_fraction": {str(f): v / (float(ops.sample_counts(G, M).sum().item()) / 2)
+                                  for f, v in b["held_out"].items()}}
+    print(json.dumps(line), flush=True)
+
+
 def run_e2e_dist(args, G_dev, P0, Q0, M_loc, N, K, prec, dev, world):
     """e2e at N GPUs: each rank's packed rows and P rows plus Q from pinned host memory,
     ``optimize_parameters_dist`` for ``steps`` iterations, P rows and Q back to the host;
@@ -913,6 +967,10 @@ def main():
     ap.add_argument("--errors", action="store_true",
                     help="per-iteration error of each E-step arithmetic against the float64 run")
     ap.add_argument("--error-iters", dest="error_iters", type=int, default=20)
+    ap.add_argument("--cv-max-iter", dest="cv_max_iter", type=int, default=200,
+                    help="c4: iteration cap of the full-data fits")
+    ap.add_argument("--cv-polish", dest="cv_polish", type=int, default=10,
+                    help="c4: Adam-EM iterations per fold")
     ap.add_argument("--kernels-skip-hessian", dest="kernels_skip_hessian", action="store_true")
     ap.add_argument("--sweep-by-k", dest="sweep_by_k", action="store_true",
                     help="float32 vs FP16 tensor-core sweep time for K = 2..16")
@@ -938,6 +996,10 @@ def main():
     if args.errors:
         if rank == 0:
             run_errors(args, cfg)
+        return
+    if args.config == "c4":
+        if rank == 0:
+            run_cv_batch(args, cfg)
         return
     if args.sweep_by_k:
         if rank == 0:

@@ -144,6 +144,30 @@ int adx_em_adam_iteration(const uint8_t* G, int64_t M, int64_t N, int K, int pre
                           double beta1, double beta2, double eps, void* workspace,
                           size_t workspace_bytes, void* stream);
 
+/* ---------------------------------------------------------------- batched float64 E-step
+ * Several Adam-EM problems on one cohort in one sweep launch: n <= 64 problems, each with its
+ * own K[p] <= 16, P[p] [M][K[p]] and Q[p] [N][K[p]] (device float64; the arrays of pointers
+ * and K/fold are HOST arrays), and a fold: entries (j, i) whose cross-validation hash
+ * h(j*N + i, seed) mod n_buckets equals fold[p] are treated as missing (fold[p] = -1: none;
+ * the hash is the reference's fold rule, adamixture/src/cv.py:58-78, so with n_buckets = 10
+ * and folds 0..4 each fold holds out 10 % of the entries). Each CTA reads a genotype tile
+ * once and runs every problem on it. Every problem's statistics are bit-identical to the
+ * single-problem float64 sweep (adx_em_stats / adx_em_adam_iteration at ADX_F64) of the
+ * same P, Q and masked genotypes. The reference runs the K sweep and its CV folds one after
+ * the other (adamixture/src/main.py:67-107, adamixture/src/cv.py:171-267); no counterpart
+ * batches them. */
+int adx_em_batch_workspace_bytes(int64_t M, int64_t N, int n, const int* K, size_t* bytes);
+int adx_em_sweep_batch(const uint8_t* G, int64_t M, int64_t N, int n, const int* K, const int* fold,
+                       uint64_t seed, int n_buckets, const double* const* P, const double* const* Q,
+                       void* workspace, size_t workspace_bytes, void* stream);
+/* Problem p of the last batched sweep in `workspace`: mode 0 writes its A, B, T (float64);
+ * mode 1 forms the EM targets and applies the Adam move to its P, Q and moments (t = step
+ * count after the increment), as adx_em_adam_iteration does. */
+int adx_em_batch_apply(int64_t M, int64_t N, int n, const int* K, int p, int mode, double* A, double* B,
+                       double* T, const double* q_bat, double* P, double* Q, double* mP, double* vP,
+                       double* mQ, double* vQ, double t, double lr, double beta1, double beta2, double eps,
+                       void* workspace, size_t workspace_bytes, void* stream);
+
 /* Binomial log-likelihood, float64 sum: sum over observed entries of
  * g log h + (2-g) log(1-h), h = clamp(P Q^T, 1e-10, 1-1e-10) (loglikelihood_gpu,
  * em_adam_gpu.py:226-279). *out is a device double. */
