@@ -92,5 +92,3 @@ def test_batched_cross_validation_equals_sequential(ops):
                 assert float((x - y).abs().max()) <= 1e-12, (K, f)
         assert abs(b["cv"][K] - s["cv"][K]) <= 1e-12 * abs(s["cv"][K]), K
     print("cv index", b["cv"], "seconds batched", b["seconds"], "sequential", s["seconds"])
-    # the simulated K has the lowest CV index
-    assert min(b["cv"], key=b["cv"].get) == 4
