@@ -695,8 +695,7 @@ extern "C" int adx_em_adam_iteration(const uint8_t* G, int64_t M, int64_t N, int
 namespace adx {
 int dmma_sweep_batch(const uint8_t* G, int64_t M, int64_t N, int n, const int* K, const int* fold,
                      const double* const* P, const double* const* Q, double* const* ABp, double* const* Tp,
-                     uint64_t seed, int n_buckets, int64_t n_stile, int n_split, int n_mblk, int64_t mb,
-                     cudaStream_t st);
+                     const uint8_t* bmap, int64_t n_stile, int n_split, int n_mblk, int64_t mb, cudaStream_t st);
 }
 
 static int batch_layout(int64_t M, int64_t N, int n, const int* K, EmPlan& pl, size_t* offs, size_t* total) {
@@ -724,24 +723,27 @@ extern "C" int adx_em_batch_workspace_bytes(int64_t M, int64_t N, int n, const i
 }
 
 extern "C" int adx_em_sweep_batch(const uint8_t* G, int64_t M, int64_t N, int n, const int* K, const int* fold,
-                                  uint64_t seed, int n_buckets, const double* const* P, const double* const* Q,
+                                  const uint8_t* bucket_map, const double* const* P, const double* const* Q,
                                   void* workspace, size_t workspace_bytes, void* stream) {
   EmPlan pl;
   size_t offs[64], total = 0;
   int rc = batch_layout(M, N, n, K, pl, offs, &total);
-  if (rc || !G || !fold || !P || !Q || !workspace || n_buckets < 1) {
-    adx_set_message("adx_em_sweep_batch: bad argument (1 <= n <= 64 problems, 1 <= K <= 16, n_buckets >= 1)");
+  if (rc || !G || !fold || !P || !Q || !workspace) {
+    adx_set_message("adx_em_sweep_batch: bad argument (1 <= n <= 64 problems, 1 <= K <= 16)");
     return rc ? rc : ADX_ERR_ARG;
   }
   if (workspace_bytes < total) { adx_set_message("adx_em_sweep_batch: workspace too small"); return ADX_ERR_WORKSPACE; }
   double* ABp[64];
   double* Tp[64];
   for (int p = 0; p < n; ++p) {
-    if (!P[p] || !Q[p] || fold[p] >= n_buckets) { adx_set_message("adx_em_sweep_batch: bad problem"); return ADX_ERR_ARG; }
+    if (!P[p] || !Q[p] || fold[p] > 254 || (fold[p] >= 0 && !bucket_map)) {
+      adx_set_message("adx_em_sweep_batch: bad problem (a fold needs the bucket map; folds 0..254)");
+      return ADX_ERR_ARG;
+    }
     ABp[p] = reinterpret_cast<double*>(static_cast<uint8_t*>(workspace) + offs[p]);
     Tp[p] = ABp[p] + (size_t)pl.n_split * (size_t)M * 2 * K[p];
   }
-  rc = dmma_sweep_batch(G, M, N, n, K, fold, P, Q, ABp, Tp, seed, n_buckets, pl.n_stile, pl.n_split, pl.n_mblk,
+  rc = dmma_sweep_batch(G, M, N, n, K, fold, P, Q, ABp, Tp, bucket_map, pl.n_stile, pl.n_split, pl.n_mblk,
                         pl.mb, as_stream(stream));
   if (rc == ADX_ERR_ARG) adx_set_message("adx_em_sweep_batch: bad problem");
   return rc;

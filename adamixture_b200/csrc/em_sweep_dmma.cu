@@ -105,8 +105,8 @@ struct Args {
   int n_split, n_mblk;
   int64_t mb;
   int vec;            // 8-byte genotype loads allowed (N % 8 == 0, G 8-byte aligned)
-  uint64_t seed;      // fold rule: entry j*N + i is held out of a problem with fold f when
-  int n_buckets;      //   fold_hash(j*N + i, seed) % n_buckets == f
+  const uint8_t* bmap;  // [M][N] cross-validation bucket of every entry (folds only)
+  int bvec;           // 8-byte bucket loads allowed (N % 8 == 0, bmap 8-byte aligned)
 };
 
 // One E-step problem: its P [M][K] and Q [N][K] (float64), its partial sums, and the fold
@@ -126,25 +126,25 @@ struct Probs {
   int n;
 };
 
-// The cross-validation hash of a flat index j*N + i (the reference's rule,
-// adamixture/src/cv.py:58-78; identical to cv::fold_hash).
-__device__ __forceinline__ uint64_t fold_hash_dm(uint64_t flat, uint64_t seed) {
-  uint64_t h = flat + seed + 0x9E3779B97F4A7C15ull;
-  h ^= h >> 30;
-  h *= 0xBF58476D1CE4E5B9ull;
-  h ^= h >> 27;
-  h *= 0x94D049BB133111EBull;
-  h ^= h >> 31;
-  return h;
+// SNP row j of the bucket map for the thread's 8 samples from s0 (one byte per entry).
+__device__ __forceinline__ uint64_t load_buckets(const uint8_t* __restrict__ bmap, int64_t N, int64_t j, int64_t s0,
+                                                 bool full8) {
+  const uint8_t* src = bmap + j * N + s0;
+  if (full8) return __ldg(reinterpret_cast<const unsigned long long*>(src));
+  uint64_t v = ~0ull;
+#pragma unroll
+  for (int u = 0; u < 8; ++u)
+    if (s0 + u < N) v = (v & ~(0xFFull << (8 * u))) | ((uint64_t)__ldg(src + u) << (8 * u));
+  return v;
 }
 
 // KS: k-steps of 4 covering every problem's K (K <= 4 KS); NK = ceil(KS / 2) column tiles
-// of 8. NB: the fold rule's bucket count as a constant (0: taken from the arguments). A
-// CTA runs, for each of its sample sub-tiles, every problem in turn over its SNP block, so
-// the block's genotype tile is read from memory once and served from cache to the others;
-// a problem's arithmetic and summation order do not depend on the other problems, on KS
-// beyond its own K, or on NB.
-template <int KS, int NB, int MAXP>
+// of 8 (registers are sized by them; a batch skips each problem's k-steps and column tiles
+// beyond its own K, which only ever add exact zeros). A CTA runs, for each of its sample
+// sub-tiles, every problem in turn over its SNP block, so the block's genotype tile is read
+// from memory once and served from cache to the others; a problem's arithmetic and
+// summation order do not depend on the other problems.
+template <int KS, int MAXP>
 __global__ void __launch_bounds__(TPB, 1) em_sweep_dmma_kernel(Args a, Probs<MAXP> ps) {
   constexpr int NK = (KS + 1) / 2;
   extern __shared__ __align__(16) double sm[];
@@ -166,6 +166,8 @@ __global__ void __launch_bounds__(TPB, 1) em_sweep_dmma_kernel(Args a, Probs<MAX
   for (int pi = 0; pi < (MAXP == 1 ? 1 : ps.n); ++pi) {
     const Prob pr = ps.p[pi];
     const int K = pr.K;
+    const int ksp = MAXP == 1 ? KS : (K + 3) >> 2;   // this problem's k-steps and column tiles
+    const int nkp = MAXP == 1 ? NK : (ksp + 1) >> 1;
     const bool first = st == split;   // this CTA's first sub-tile: AB_part rows are written
     const int64_t i0 = st * W;
     // Q rows of the sub-tile (zero beyond N and K); the previous sub-tile's last reads of
@@ -211,15 +213,12 @@ __global__ void __launch_bounds__(TPB, 1) em_sweep_dmma_kernel(Args a, Probs<MAX
           // SNPs past the block end are missing (code 3)
           if (jc + g + 8 * h >= j1) w[h] |= 0x0303030303030303ull << (2 * (g & 3));
           w[h] >>= 2 * (g & 3);
-          // the problem's held-out entries are missing too
-          if (pr.fold >= 0) {
-            const uint64_t flat0 = (uint64_t)(jc + g + 8 * h) * (uint64_t)N + (uint64_t)s0;
-#pragma unroll
-            for (int u = 0; u < 8; ++u) {
-              const uint64_t hv = fold_hash_dm(flat0 + u, a.seed);
-              const uint64_t b = NB > 0 ? hv % (uint64_t)NB : hv % (uint64_t)a.n_buckets;
-              if (b == (uint64_t)pr.fold) w[h] |= 3ull << (8 * u);
-            }
+          // the problem's held-out entries (bucket == fold) are missing too
+          if (MAXP > 1 && pr.fold >= 0 && jc + g + 8 * h < j1) {
+            const uint64_t bk = load_buckets(a.bmap, N, jc + g + 8 * h, s0, a.bvec && s0 + 8 <= N);
+            const uint32_t f4 = 0x01010101u * (uint32_t)pr.fold;
+            const uint32_t lo = __vcmpeq4((uint32_t)bk, f4), hi = __vcmpeq4((uint32_t)(bk >> 32), f4);
+            w[h] |= (((uint64_t)hi << 32) | lo) & 0x0303030303030303ull;
           }
         }
         // this thread's two A/B partial sums of the chunk, read now so that the read's
@@ -240,8 +239,8 @@ __global__ void __launch_bounds__(TPB, 1) em_sweep_dmma_kernel(Args a, Probs<MAX
         double ph[KS][2];
 #pragma unroll
         for (int ks = 0; ks < KS; ++ks) {
-          ph[ks][0] = pc[g * PSTR + 4 * ks + t];
-          ph[ks][1] = pc[(g + 8) * PSTR + 4 * ks + t];
+          ph[ks][0] = ks < ksp ? pc[g * PSTR + 4 * ks + t] : 0.0;
+          ph[ks][1] = ks < ksp ? pc[(g + 8) * PSTR + 4 * ks + t] : 0.0;
         }
         double aacc[NK][4], bacc[NK][4];
 #pragma unroll
@@ -255,7 +254,7 @@ __global__ void __launch_bounds__(TPB, 1) em_sweep_dmma_kernel(Args a, Probs<MAX
           const int qrow_h = warp * WS + 8 * (g >> 1) + (g & 1);
 #pragma unroll
           for (int ks = 0; ks < KS; ++ks)
-            mma_f64(hcur, ph[ks][0], ph[ks][1], qt[qrow_h * QSTR + ((4 * ks + t) ^ qsw(qrow_h))]);
+            if (ks < ksp) mma_f64(hcur, ph[ks][0], ph[ks][1], qt[qrow_h * QSTR + ((4 * ks + t) ^ qsw(qrow_h))]);
         }
 #pragma unroll
         for (int nt = 0; nt < 4; ++nt) {
@@ -265,7 +264,7 @@ __global__ void __launch_bounds__(TPB, 1) em_sweep_dmma_kernel(Args a, Probs<MAX
             hnext[0] = hnext[1] = hnext[2] = hnext[3] = 0.0;
 #pragma unroll
             for (int ks = 0; ks < KS; ++ks)
-              mma_f64(hnext, ph[ks][0], ph[ks][1], qt[qrow_h * QSTR + ((4 * ks + t) ^ qsw(qrow_h))]);
+              if (ks < ksp) mma_f64(hnext, ph[ks][0], ph[ks][1], qt[qrow_h * QSTR + ((4 * ks + t) ^ qsw(qrow_h))]);
           }
           const double (&hacc)[4] = hcur;
           double av[4], bv[4];
@@ -297,6 +296,7 @@ __global__ void __launch_bounds__(TPB, 1) em_sweep_dmma_kernel(Args a, Probs<MAX
             const int qrow = warp * WS + 8 * t + 2 * nt + c;
 #pragma unroll
             for (int n = 0; n < NK; ++n) {
+              if (n >= nkp) continue;
               const double qb = qt[qrow * QSTR + ((8 * n + g) ^ qsw(qrow))];
               mma_f64(aacc[n], av[c], av[2 + c], qb);
               mma_f64(bacc[n], bv[c], bv[2 + c], qb);
@@ -320,7 +320,8 @@ __global__ void __launch_bounds__(TPB, 1) em_sweep_dmma_kernel(Args a, Probs<MAX
             const double d0 = dT[r0 * DSTR + ((4 * q + t) ^ dsw(r0))];
             const double d1 = dT[r1 * DSTR + ((4 * q + t) ^ dsw(r1))];
 #pragma unroll
-            for (int n = 0; n < NK; ++n) mma_f64(tacc[m][n], d0, d1, pb[n]);
+            for (int n = 0; n < NK; ++n)
+              if (n < nkp) mma_f64(tacc[m][n], d0, d1, pb[n]);
           }
         }
         // A/B of the chunk: this warp's share into the reduction buffer
@@ -340,7 +341,7 @@ __global__ void __launch_bounds__(TPB, 1) em_sweep_dmma_kernel(Args a, Probs<MAX
           const int e = threadIdx.x + u * TPB;
           const int v = e >> 5, l = e & 31;
           const int n = (v >> 2) & 1;
-          if (n >= NK) continue;
+          if (n >= nkp) continue;
           const int el = v & 3;
           const int row = (l >> 2) + 8 * (el >> 1);
           const int col = 8 * n + 2 * (l & 3) + (el & 1);
@@ -403,17 +404,17 @@ __global__ void __launch_bounds__(TPB, 1) em_sweep_dmma_kernel(Args a, Probs<MAX
 int dmma_plan_width() { return dm::W; }
 int dmma_plan_chunk() { return dm::CH; }
 
-template <int KS, int NB, int MAXP>
+template <int KS, int MAXP>
 static int dmma_launch(const dm::Args& a, const dm::Probs<MAXP>& ps, cudaStream_t st) {
   static bool attr_set[64] = {false};
   int dev = 0;
   ADX_CUDA_TRY(cudaGetDevice(&dev));
   if (dev >= 0 && dev < 64 && !attr_set[dev]) {
-    ADX_CUDA_TRY(cudaFuncSetAttribute(dm::em_sweep_dmma_kernel<KS, NB, MAXP>,
+    ADX_CUDA_TRY(cudaFuncSetAttribute(dm::em_sweep_dmma_kernel<KS, MAXP>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dm::SMEM_BYTES));
     attr_set[dev] = true;
   }
-  dm::em_sweep_dmma_kernel<KS, NB, MAXP><<<(unsigned)(a.n_split * a.n_mblk), dm::TPB, dm::SMEM_BYTES, st>>>(a, ps);
+  dm::em_sweep_dmma_kernel<KS, MAXP><<<(unsigned)(a.n_split * a.n_mblk), dm::TPB, dm::SMEM_BYTES, st>>>(a, ps);
   ADX_LAUNCH_CHECK();
   return ADX_OK;
 }
@@ -426,15 +427,15 @@ int dmma_sweep(const uint8_t* G, const double* P, const double* Q, int64_t M, in
                int64_t n_stile, int n_split, int n_mblk, int64_t mb, double* ABp, double* Tp,
                cudaStream_t st) {
   if (K < 1 || K > 16) return ADX_ERR_UNSUPPORTED;
-  const dm::Args a{G, M, N, n_stile, n_split, n_mblk, mb, dmma_vec(G, N), 0, 0};
+  const dm::Args a{G, M, N, n_stile, n_split, n_mblk, mb, dmma_vec(G, N), nullptr, 0};
   dm::Probs<1> ps;
   ps.p[0] = dm::Prob{P, Q, ABp, Tp, K, -1};
   ps.n = 1;
   switch ((K + 3) / 4) {
-    case 1: return dmma_launch<1, 0, 1>(a, ps, st);
-    case 2: return dmma_launch<2, 0, 1>(a, ps, st);
-    case 3: return dmma_launch<3, 0, 1>(a, ps, st);
-    default: return dmma_launch<4, 0, 1>(a, ps, st);
+    case 1: return dmma_launch<1, 1>(a, ps, st);
+    case 2: return dmma_launch<2, 1>(a, ps, st);
+    case 3: return dmma_launch<3, 1>(a, ps, st);
+    default: return dmma_launch<4, 1>(a, ps, st);
   }
 }
 
@@ -442,27 +443,24 @@ constexpr int DMMA_MAX_PROBLEMS = 64;
 
 int dmma_sweep_batch(const uint8_t* G, int64_t M, int64_t N, int n, const int* K, const int* fold,
                      const double* const* P, const double* const* Q, double* const* ABp, double* const* Tp,
-                     uint64_t seed, int n_buckets, int64_t n_stile, int n_split, int n_mblk, int64_t mb,
-                     cudaStream_t st) {
-  if (n < 1 || n > DMMA_MAX_PROBLEMS || n_buckets < 1) return ADX_ERR_ARG;
-  const dm::Args a{G, M, N, n_stile, n_split, n_mblk, mb, dmma_vec(G, N), seed, n_buckets};
+                     const uint8_t* bmap, int64_t n_stile, int n_split, int n_mblk, int64_t mb, cudaStream_t st) {
+  if (n < 1 || n > DMMA_MAX_PROBLEMS) return ADX_ERR_ARG;
+  const int bvec = ((N & 7) == 0 && (reinterpret_cast<uintptr_t>(bmap) & 7) == 0) ? 1 : 0;
+  const dm::Args a{G, M, N, n_stile, n_split, n_mblk, mb, dmma_vec(G, N), bmap, bvec};
   dm::Probs<DMMA_MAX_PROBLEMS> ps;
   int kmax = 1;
   for (int p = 0; p < n; ++p) {
-    if (K[p] < 1 || K[p] > 16 || fold[p] >= n_buckets) return ADX_ERR_ARG;
+    if (K[p] < 1 || K[p] > 16 || fold[p] > 254 || (fold[p] >= 0 && !bmap)) return ADX_ERR_ARG;
     ps.p[p] = dm::Prob{P[p], Q[p], ABp[p], Tp[p], K[p], fold[p] < 0 ? -1 : fold[p]};
     kmax = K[p] > kmax ? K[p] : kmax;
   }
   ps.n = n;
-  const bool ten = n_buckets == 10;
-#define ADX_DM_BATCH(KS) return ten ? dmma_launch<KS, 10, DMMA_MAX_PROBLEMS>(a, ps, st) : dmma_launch<KS, 0, DMMA_MAX_PROBLEMS>(a, ps, st)
   switch ((kmax + 3) / 4) {
-    case 1: ADX_DM_BATCH(1);
-    case 2: ADX_DM_BATCH(2);
-    case 3: ADX_DM_BATCH(3);
-    default: ADX_DM_BATCH(4);
+    case 1: return dmma_launch<1, DMMA_MAX_PROBLEMS>(a, ps, st);
+    case 2: return dmma_launch<2, DMMA_MAX_PROBLEMS>(a, ps, st);
+    case 3: return dmma_launch<3, DMMA_MAX_PROBLEMS>(a, ps, st);
+    default: return dmma_launch<4, DMMA_MAX_PROBLEMS>(a, ps, st);
   }
-#undef ADX_DM_BATCH
 }
 
 }  // namespace adx

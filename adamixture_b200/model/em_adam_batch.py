@@ -9,7 +9,9 @@ tile once and runs every problem on it), then each problem's EM targets and Adam
 
 Fold rule: entry (j, i) belongs to bucket ``h(j*N + i, seed) mod n_buckets`` with h the
 reference's cross-validation hash (cv.py:58-78); fold f holds out bucket f. With
-``n_buckets=10`` and folds 0..4, each fold masks 10 % of the entries.
+``n_buckets=10`` and folds 0..4, each fold masks 10 % of the entries. The buckets are
+evaluated once per run into an [M, N] byte map that the batched sweep reads beside the
+genotypes (M*N bytes of device memory: 2 GB at N=20,000, M=100,000).
 
 Every problem follows exactly the single-problem path's arithmetic and control flow
 (``optimize_parameters_gpu`` at float64 for full-data problems; plain Adam-EM iterations
@@ -79,9 +81,9 @@ def _prepare(G, M, problems, seed, n_buckets):
         pr.q_bat = counts[pr.fold]
 
 
-def _iteration(G, M, N, live, seed, n_buckets):
+def _iteration(G, M, N, live, bmap):
     """One batched sweep over the live problems, then each one's targets + Adam move."""
-    batch = ops.EmBatch(M, N, [p.K for p in live], [p.fold for p in live], seed, n_buckets, G.device)
+    batch = ops.EmBatch(M, N, [p.K for p in live], [p.fold for p in live], bmap, G.device)
     batch.sweep(G, [p.P for p in live], [p.Q for p in live])
     for k, pr in enumerate(live):
         pr.t += 1.0
@@ -102,16 +104,17 @@ def optimize_batch(G, M, N, problems, seed=0, n_buckets=10, max_iter=10000, chec
     n Adam-EM iterations (the first one from the start) and keeps its last iterate.
     Returns the problems (results in ``P_best``/``Q_best``)."""
     _prepare(G, M, problems, seed, n_buckets)
+    bmap = ops.cv_bucket_map(M, N, seed, n_buckets, G.device) if any(p.fold >= 0 for p in problems) else None
     if fixed_iters is not None:
         for _ in range(int(fixed_iters)):
-            _iteration(G, M, N, problems, seed, n_buckets)
+            _iteration(G, M, N, problems, bmap)
         for pr in problems:
             pr.P_best, pr.Q_best = pr.P, pr.Q
         return problems
     if any(p.fold >= 0 for p in problems):
         raise ValueError("fold problems run a fixed number of iterations (fixed_iters)")
     # priming: one iteration, then the primed point's log-likelihood is the first best
-    _iteration(G, M, N, problems, seed, n_buckets)
+    _iteration(G, M, N, problems, bmap)
     for pr in problems:
         pr.L_best = float(ops.loglik_device(G, pr.P, pr.Q, M, "f64").item())
         pr.P_best, pr.Q_best = pr.P.clone(), pr.Q.clone()
@@ -119,7 +122,7 @@ def optimize_batch(G, M, N, problems, seed=0, n_buckets=10, max_iter=10000, chec
         live = [p for p in problems if p.active]
         if not live:
             break
-        _iteration(G, M, N, live, seed, n_buckets)
+        _iteration(G, M, N, live, bmap)
         if (it + 1) % check:
             continue
         for pr in live:

@@ -245,14 +245,17 @@ class EmBatch:
     """Host-side description of a batch of float64 E-step problems on one cohort (the
     C arrays the batch entry points take) and its partial-sum workspace."""
 
-    def __init__(self, M: int, N: int, Ks, folds, seed: int = 0, n_buckets: int = 10, device=None):
+    def __init__(self, M: int, N: int, Ks, folds, bucket_map: torch.Tensor | None = None, device=None):
         import ctypes
 
         self.M, self.N = int(M), int(N)
         self.n = len(Ks)
         self.K = (ctypes.c_int * self.n)(*[int(k) for k in Ks])
         self.fold = (ctypes.c_int * self.n)(*[int(f) for f in folds])
-        self.seed, self.n_buckets = int(seed), int(n_buckets)
+        if any(int(f) >= 0 for f in folds):
+            if bucket_map is None or bucket_map.shape != (self.M, self.N) or bucket_map.dtype != torch.uint8:
+                raise ValueError("fold problems need the [M, N] uint8 bucket map (cv_bucket_map)")
+        self.bucket_map = bucket_map
         nbytes = query_size("adx_em_batch_workspace_bytes", self.M, self.N, self.n, ctypes.addressof(self.K))
         dev = torch.device("cuda", torch.cuda.current_device()) if device is None else torch.device(device)
         self.workspace = Workspace.get(dev, nbytes, tag="em_batch")
@@ -270,7 +273,7 @@ class EmBatch:
         pp = (ctypes.c_void_p * self.n)(*[P.data_ptr() for P in Ps])
         qq = (ctypes.c_void_p * self.n)(*[Q.data_ptr() for Q in Qs])
         call("adx_em_sweep_batch", G.data_ptr(), self.M, self.N, self.n, ctypes.addressof(self.K),
-             ctypes.addressof(self.fold), self.seed, self.n_buckets, ctypes.addressof(pp), ctypes.addressof(qq),
+             ctypes.addressof(self.fold), _ptr(self.bucket_map), ctypes.addressof(pp), ctypes.addressof(qq),
              self.workspace.data_ptr(), self.workspace.numel(), _stream(G.device))
 
     def stats(self, p: int):
@@ -295,6 +298,14 @@ class EmBatch:
              q_bat.data_ptr(), P.data_ptr(), Q.data_ptr(), mP.data_ptr(), vP.data_ptr(), mQ.data_ptr(),
              vQ.data_ptr(), float(t), float(lr), float(beta1), float(beta2), float(eps),
              self.workspace.data_ptr(), self.workspace.numel(), _stream(P.device))
+
+
+def cv_bucket_map(M: int, N: int, seed: int, n_buckets: int, device=None) -> torch.Tensor:
+    """[M, N] uint8: the hash fold rule's bucket of every entry."""
+    dev = torch.device("cuda", torch.cuda.current_device()) if device is None else torch.device(device)
+    out = torch.empty((M, N), dtype=torch.uint8, device=dev)
+    call("adx_cv_bucket_map", M, N, int(seed) & 0xFFFFFFFFFFFFFFFF, int(n_buckets), out.data_ptr(), _stream(dev))
+    return out
 
 
 def loglik_device(G: torch.Tensor, P: torch.Tensor, Q: torch.Tensor, M: int, precision="f64",

@@ -44,7 +44,7 @@ def test_batched_stats_equal_single_problem_sweeps(ops, N, M):
     folds = [-1, 0, 3, -1, 9, 4]
     seed = 42
     starts = [_start(M, N, K, 10 + i) for i, K in enumerate(Ks)]
-    batch = ops.EmBatch(M, N, Ks, folds, seed, 10, G.device)
+    batch = ops.EmBatch(M, N, Ks, folds, ops.cv_bucket_map(M, N, seed, 10), G.device)
     batch.sweep(G, [s[0] for s in starts], [s[1] for s in starts])
     for p, (K, f) in enumerate(zip(Ks, folds)):
         A, B, T = batch.stats(p)
