@@ -42,8 +42,7 @@ SIGNATURES: dict[str, list] = {
     "adx_em_adam_iteration": [P, I64, I64, c_int, c_int, P, P, P, P, P, P, P, P, P, c_double,
                               c_double, c_double, c_double, c_double, P, c_size_t, P],
     "adx_em_batch_workspace_bytes": [I64, I64, c_int, P, P],
-    "adx_em_sweep_batch": [P, I64, I64, c_int, P, P, P, P, P, P, c_size_t, P],
-    "adx_cv_bucket_map": [I64, I64, c_uint64, c_int, P, P],
+    "adx_em_sweep_batch": [I64, I64, c_int, P, P, P, P, P, c_size_t, P],
     "adx_em_batch_apply": [I64, I64, c_int, P, c_int, c_int, P, P, P, P, P, P, P, P, P, P, c_double,
                            c_double, c_double, c_double, c_double, P, c_size_t, P],
     "adx_loglik_workspace_bytes": [I64, I64, c_int, c_int, P],

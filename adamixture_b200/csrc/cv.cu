@@ -142,16 +142,6 @@ __global__ void __launch_bounds__(TPB) dev_hash_kernel(const uint8_t* __restrict
   block_sum_to(acc, part);
 }
 
-// map[j*N + i] = fold_hash(j*N + i, seed) % n_buckets: the bucket of every entry, for
-// problems that hold out one bucket (NF > 0: the bucket count as a constant).
-template <int NF>
-__global__ void bucket_map_kernel(int64_t n, uint64_t seed, uint64_t n_buckets, uint8_t* __restrict__ map) {
-  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
-    const uint64_t h = fold_hash((uint64_t)e, seed);
-    map[e] = (uint8_t)(NF > 0 ? h % (uint64_t)NF : h % n_buckets);
-  }
-}
-
 __global__ void sum_kernel(const double* part, int n, double* out) {
   if (threadIdx.x == 0 && blockIdx.x == 0) {
     double s = 0.0;
@@ -270,16 +260,3 @@ extern "C" int adx_cv_deviance_hash(const uint8_t* G0, int64_t M, int64_t N, int
   return ADX_OK;
 }
 
-extern "C" int adx_cv_bucket_map(int64_t M, int64_t N, uint64_t seed, int n_buckets, uint8_t* map, void* stream) {
-  if (M <= 0 || N <= 0 || !map || n_buckets < 1 || n_buckets > 255) {
-    adx_set_message("adx_cv_bucket_map: bad argument (1 <= n_buckets <= 255)");
-    return ADX_ERR_ARG;
-  }
-  const int64_t blocks = (int64_t)sm_count() * 16;
-  cudaStream_t st = as_stream(stream);
-#define ADX_BMAP(NF) cv::bucket_map_kernel<NF><<<(unsigned)blocks, 256, 0, st>>>(M * N, seed, (uint64_t)n_buckets, map)
-  ADX_CV_FOLD_SWITCH(n_buckets, ADX_BMAP)
-#undef ADX_BMAP
-  ADX_LAUNCH_CHECK();
-  return ADX_OK;
-}

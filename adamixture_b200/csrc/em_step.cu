@@ -693,9 +693,9 @@ extern "C" int adx_em_adam_iteration(const uint8_t* G, int64_t M, int64_t N, int
 // and T partials, each 256-byte aligned.
 
 namespace adx {
-int dmma_sweep_batch(const uint8_t* G, int64_t M, int64_t N, int n, const int* K, const int* fold,
-                     const double* const* P, const double* const* Q, double* const* ABp, double* const* Tp,
-                     const uint8_t* bmap, int64_t n_stile, int n_split, int n_mblk, int64_t mb, cudaStream_t st);
+int dmma_sweep_batch(int64_t M, int64_t N, int n, const int* K, const uint8_t* const* G, const double* const* P,
+                     const double* const* Q, double* const* ABp, double* const* Tp, int64_t n_stile, int n_split,
+                     int n_mblk, int64_t mb, cudaStream_t st);
 }
 
 static int batch_layout(int64_t M, int64_t N, int n, const int* K, EmPlan& pl, size_t* offs, size_t* total) {
@@ -722,13 +722,13 @@ extern "C" int adx_em_batch_workspace_bytes(int64_t M, int64_t N, int n, const i
   return rc;
 }
 
-extern "C" int adx_em_sweep_batch(const uint8_t* G, int64_t M, int64_t N, int n, const int* K, const int* fold,
-                                  const uint8_t* bucket_map, const double* const* P, const double* const* Q,
-                                  void* workspace, size_t workspace_bytes, void* stream) {
+extern "C" int adx_em_sweep_batch(int64_t M, int64_t N, int n, const int* K, const uint8_t* const* G,
+                                  const double* const* P, const double* const* Q, void* workspace,
+                                  size_t workspace_bytes, void* stream) {
   EmPlan pl;
   size_t offs[64], total = 0;
   int rc = batch_layout(M, N, n, K, pl, offs, &total);
-  if (rc || !G || !fold || !P || !Q || !workspace) {
+  if (rc || !G || !P || !Q || !workspace) {
     adx_set_message("adx_em_sweep_batch: bad argument (1 <= n <= 64 problems, 1 <= K <= 16)");
     return rc ? rc : ADX_ERR_ARG;
   }
@@ -736,17 +736,12 @@ extern "C" int adx_em_sweep_batch(const uint8_t* G, int64_t M, int64_t N, int n,
   double* ABp[64];
   double* Tp[64];
   for (int p = 0; p < n; ++p) {
-    if (!P[p] || !Q[p] || fold[p] > 254 || (fold[p] >= 0 && !bucket_map)) {
-      adx_set_message("adx_em_sweep_batch: bad problem (a fold needs the bucket map; folds 0..254)");
-      return ADX_ERR_ARG;
-    }
+    if (!G[p] || !P[p] || !Q[p]) { adx_set_message("adx_em_sweep_batch: null pointer"); return ADX_ERR_ARG; }
     ABp[p] = reinterpret_cast<double*>(static_cast<uint8_t*>(workspace) + offs[p]);
     Tp[p] = ABp[p] + (size_t)pl.n_split * (size_t)M * 2 * K[p];
   }
-  rc = dmma_sweep_batch(G, M, N, n, K, fold, P, Q, ABp, Tp, bucket_map, pl.n_stile, pl.n_split, pl.n_mblk,
-                        pl.mb, as_stream(stream));
-  if (rc == ADX_ERR_ARG) adx_set_message("adx_em_sweep_batch: bad problem");
-  return rc;
+  return dmma_sweep_batch(M, N, n, K, G, P, Q, ABp, Tp, pl.n_stile, pl.n_split, pl.n_mblk, pl.mb,
+                          as_stream(stream));
 }
 
 extern "C" int adx_em_batch_apply(int64_t M, int64_t N, int n, const int* K, int p, int mode, double* A, double* B,

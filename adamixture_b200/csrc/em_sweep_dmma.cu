@@ -99,25 +99,22 @@ __device__ __forceinline__ void load_words(const uint8_t* __restrict__ G, int64_
 }
 
 struct Args {
-  const uint8_t* G;
   int64_t M, N;
   int64_t n_stile;
   int n_split, n_mblk;
   int64_t mb;
-  int vec;            // 8-byte genotype loads allowed (N % 8 == 0, G 8-byte aligned)
-  const uint8_t* bmap;  // [M][N] cross-validation bucket of every entry (folds only)
-  int bvec;           // 8-byte bucket loads allowed (N % 8 == 0, bmap 8-byte aligned)
 };
 
-// One E-step problem: its P [M][K] and Q [N][K] (float64), its partial sums, and the fold
-// whose entries it treats as missing (-1: none).
+// One E-step problem: its packed genotypes (cross-validation folds pass a copy with the
+// fold's entries hidden), P [M][K] and Q [N][K] (float64), and its partial sums.
 struct Prob {
+  const uint8_t* G;
   const double* P;
   const double* Q;
   double* ABp;
   double* Tp;
   int K;
-  int fold;
+  int vec;            // 8-byte genotype loads allowed (N % 8 == 0, G 8-byte aligned)
 };
 
 template <int MAXP>
@@ -126,23 +123,12 @@ struct Probs {
   int n;
 };
 
-// SNP row j of the bucket map for the thread's 8 samples from s0 (one byte per entry).
-__device__ __forceinline__ uint64_t load_buckets(const uint8_t* __restrict__ bmap, int64_t N, int64_t j, int64_t s0,
-                                                 bool full8) {
-  const uint8_t* src = bmap + j * N + s0;
-  if (full8) return __ldg(reinterpret_cast<const unsigned long long*>(src));
-  uint64_t v = ~0ull;
-#pragma unroll
-  for (int u = 0; u < 8; ++u)
-    if (s0 + u < N) v = (v & ~(0xFFull << (8 * u))) | ((uint64_t)__ldg(src + u) << (8 * u));
-  return v;
-}
-
 // KS: k-steps of 4 covering every problem's K (K <= 4 KS); NK = ceil(KS / 2) column tiles
 // of 8 (registers are sized by them; a batch skips each problem's k-steps and column tiles
-// beyond its own K, which only ever add exact zeros). A CTA runs, for each of its sample
-// sub-tiles, every problem in turn over its SNP block, so the block's genotype tile is read
-// from memory once and served from cache to the others; a problem's arithmetic and
+// beyond its own K, which only ever add exact zeros). A CTA runs the problems in order,
+// each over the CTA's whole share of the matrix (its SNP block x its sample sub-tiles), so
+// consecutive problems on the same genotypes find the CTA's genotype region (about 0.3 MB
+// at N=20k, M=100k) still in L2 and read it from memory once; a problem's arithmetic and
 // summation order do not depend on the other problems.
 template <int KS, int MAXP>
 __global__ void __launch_bounds__(TPB, 1) em_sweep_dmma_kernel(Args a, Probs<MAXP> ps) {
@@ -162,8 +148,8 @@ __global__ void __launch_bounds__(TPB, 1) em_sweep_dmma_kernel(Args a, Probs<MAX
   const int64_t rows = (M + 3) >> 2;
   int chunk_no = 0;   // parity of the A/B reduction buffer
 
-  for (int64_t st = split; st < a.n_stile; st += a.n_split)
-  for (int pi = 0; pi < (MAXP == 1 ? 1 : ps.n); ++pi) {
+  for (int pi = 0; pi < (MAXP == 1 ? 1 : ps.n); ++pi)
+  for (int64_t st = split; st < a.n_stile; st += a.n_split) {
     const Prob pr = ps.p[pi];
     const int K = pr.K;
     const int ksp = MAXP == 1 ? KS : (K + 3) >> 2;   // this problem's k-steps and column tiles
@@ -191,9 +177,9 @@ __global__ void __launch_bounds__(TPB, 1) em_sweep_dmma_kernel(Args a, Probs<MAX
     // this thread's 8 consecutive samples; the first chunk's genotype words are loaded
     // here and each chunk loads the next one's, a chunk ahead of their use
     const int64_t s0 = i0 + warp * WS + 8 * t;
-    const bool full8 = a.vec && (s0 + 8 <= N);
+    const bool full8 = pr.vec && (s0 + 8 <= N);
     uint64_t wnext[2];
-    load_words(a.G, N, rows, j0, g, s0, full8, wnext);
+    load_words(pr.G, N, rows, j0, g, s0, full8, wnext);
 
     for (int64_t gj = j0; gj < j1; gj += GS) {
       const int gn = (int)min((int64_t)GS, j1 - gj);
@@ -207,19 +193,12 @@ __global__ void __launch_bounds__(TPB, 1) em_sweep_dmma_kernel(Args a, Probs<MAX
         const int64_t jc = gj + ch * CH;
         const double* pc = pt + ch * CH * PSTR;
         uint64_t w[2] = {wnext[0], wnext[1]};
-        if (jc + CH < j1) load_words(a.G, N, rows, jc + CH, g, s0, full8, wnext);
+        if (jc + CH < j1) load_words(pr.G, N, rows, jc + CH, g, s0, full8, wnext);
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
           // SNPs past the block end are missing (code 3)
           if (jc + g + 8 * h >= j1) w[h] |= 0x0303030303030303ull << (2 * (g & 3));
           w[h] >>= 2 * (g & 3);
-          // the problem's held-out entries (bucket == fold) are missing too
-          if (MAXP > 1 && pr.fold >= 0 && jc + g + 8 * h < j1) {
-            const uint64_t bk = load_buckets(a.bmap, N, jc + g + 8 * h, s0, a.bvec && s0 + 8 <= N);
-            const uint32_t f4 = 0x01010101u * (uint32_t)pr.fold;
-            const uint32_t lo = __vcmpeq4((uint32_t)bk, f4), hi = __vcmpeq4((uint32_t)(bk >> 32), f4);
-            w[h] |= (((uint64_t)hi << 32) | lo) & 0x0303030303030303ull;
-          }
         }
         // this thread's two A/B partial sums of the chunk, read now so that the read's
         // latency overlaps the chunk's arithmetic (added after the chunk barrier)
@@ -427,9 +406,9 @@ int dmma_sweep(const uint8_t* G, const double* P, const double* Q, int64_t M, in
                int64_t n_stile, int n_split, int n_mblk, int64_t mb, double* ABp, double* Tp,
                cudaStream_t st) {
   if (K < 1 || K > 16) return ADX_ERR_UNSUPPORTED;
-  const dm::Args a{G, M, N, n_stile, n_split, n_mblk, mb, dmma_vec(G, N), nullptr, 0};
+  const dm::Args a{M, N, n_stile, n_split, n_mblk, mb};
   dm::Probs<1> ps;
-  ps.p[0] = dm::Prob{P, Q, ABp, Tp, K, -1};
+  ps.p[0] = dm::Prob{G, P, Q, ABp, Tp, K, dmma_vec(G, N)};
   ps.n = 1;
   switch ((K + 3) / 4) {
     case 1: return dmma_launch<1, 1>(a, ps, st);
@@ -441,17 +420,16 @@ int dmma_sweep(const uint8_t* G, const double* P, const double* Q, int64_t M, in
 
 constexpr int DMMA_MAX_PROBLEMS = 64;
 
-int dmma_sweep_batch(const uint8_t* G, int64_t M, int64_t N, int n, const int* K, const int* fold,
-                     const double* const* P, const double* const* Q, double* const* ABp, double* const* Tp,
-                     const uint8_t* bmap, int64_t n_stile, int n_split, int n_mblk, int64_t mb, cudaStream_t st) {
+int dmma_sweep_batch(int64_t M, int64_t N, int n, const int* K, const uint8_t* const* G, const double* const* P,
+                     const double* const* Q, double* const* ABp, double* const* Tp, int64_t n_stile, int n_split,
+                     int n_mblk, int64_t mb, cudaStream_t st) {
   if (n < 1 || n > DMMA_MAX_PROBLEMS) return ADX_ERR_ARG;
-  const int bvec = ((N & 7) == 0 && (reinterpret_cast<uintptr_t>(bmap) & 7) == 0) ? 1 : 0;
-  const dm::Args a{G, M, N, n_stile, n_split, n_mblk, mb, dmma_vec(G, N), bmap, bvec};
+  const dm::Args a{M, N, n_stile, n_split, n_mblk, mb};
   dm::Probs<DMMA_MAX_PROBLEMS> ps;
   int kmax = 1;
   for (int p = 0; p < n; ++p) {
-    if (K[p] < 1 || K[p] > 16 || fold[p] > 254 || (fold[p] >= 0 && !bmap)) return ADX_ERR_ARG;
-    ps.p[p] = dm::Prob{P[p], Q[p], ABp[p], Tp[p], K[p], fold[p] < 0 ? -1 : fold[p]};
+    if (K[p] < 1 || K[p] > 16 || !G[p]) return ADX_ERR_ARG;
+    ps.p[p] = dm::Prob{G[p], P[p], Q[p], ABp[p], Tp[p], K[p], dmma_vec(G[p], N)};
     kmax = K[p] > kmax ? K[p] : kmax;
   }
   ps.n = n;

@@ -4,20 +4,21 @@ The reference runs the K sweep one K at a time (adamixture/src/main.py:67-107) a
 cross-validation per K and fold afterwards (adamixture/src/cv.py:171-267). Here a list of
 problems -- each with its own K (<= 16), start, Adam state and learning-rate schedule, and
 optionally a cross-validation fold whose entries it treats as missing -- advances together:
-every iteration is ONE launch of the batched float64 E-step sweep (each CTA reads a genotype
-tile once and runs every problem on it), then each problem's EM targets and Adam move.
+every iteration is ONE launch of the batched float64 E-step sweep, then each problem's EM
+targets and Adam move. Each CTA of the sweep runs the problems in order over its share of
+the matrix, so problems on the same genotypes (all full-data fits; all problems of one
+fold) read them from memory once and from L2 after that.
 
 Fold rule: entry (j, i) belongs to bucket ``h(j*N + i, seed) mod n_buckets`` with h the
 reference's cross-validation hash (cv.py:58-78); fold f holds out bucket f. With
-``n_buckets=10`` and folds 0..4, each fold masks 10 % of the entries. The buckets are
-evaluated once per run into an [M, N] byte map that the batched sweep reads beside the
-genotypes (M*N bytes of device memory: 2 GB at N=20,000, M=100,000).
+``n_buckets=10`` and folds 0..4, each fold masks 10 % of the entries. A fold's problems
+share one copy of the packed matrix with the fold's entries hidden.
 
 Every problem follows exactly the single-problem path's arithmetic and control flow
 (``optimize_parameters_gpu`` at float64 for full-data problems; plain Adam-EM iterations
 for fold problems), so its results are bit-identical to running it alone on the same
 (masked) genotypes -- ``cross_validate(..., batched=False)`` does exactly that, through
-the single-problem kernels and a masked copy of the matrix, for comparison.
+the single-problem kernels, for comparison.
 """
 from __future__ import annotations
 
@@ -49,6 +50,7 @@ class Problem:
     mQ: torch.Tensor | None = None
     vQ: torch.Tensor | None = None
     q_bat: torch.Tensor | None = None
+    G: torch.Tensor | None = None
     t: float = 0.0
     lr: float = HP["lr"]
     L_best: float = float("-inf")
@@ -60,31 +62,36 @@ class Problem:
     trace: list = field(default_factory=list)
 
 
-def fold_counts(G: torch.Tensor, M: int, seed: int, n_buckets: int, fold: int) -> torch.Tensor:
-    """q_bat of the genotypes with fold ``fold`` hidden: 2 x observed entries per sample."""
+def fold_copy(G: torch.Tensor, M: int, seed: int, n_buckets: int, fold: int) -> torch.Tensor:
+    """A copy of the packed genotypes with bucket ``fold`` of the hash rule hidden."""
     Gm = ops.masked_copy(G)
     ops.cv_mask_hash(Gm, G, M, seed, n_buckets, fold)
-    q = ops.sample_counts(Gm, M)
-    del Gm
-    return q
+    return Gm
+
+
+def fold_counts(G: torch.Tensor, M: int, seed: int, n_buckets: int, fold: int) -> torch.Tensor:
+    """q_bat of the genotypes with fold ``fold`` hidden: 2 x observed entries per sample."""
+    return ops.sample_counts(fold_copy(G, M, seed, n_buckets, fold), M)
 
 
 def _prepare(G, M, problems, seed, n_buckets):
-    counts = {}
+    """Start state of every problem; each fold's masked copy and counts made once."""
+    shared = {}
     for pr in problems:
         pr.P = pr.P.to(torch.float64).contiguous().clone()
         pr.Q = pr.Q.to(torch.float64).contiguous().clone()
         pr.mP, pr.vP = torch.zeros_like(pr.P), torch.zeros_like(pr.P)
         pr.mQ, pr.vQ = torch.zeros_like(pr.Q), torch.zeros_like(pr.Q)
-        if pr.fold not in counts:
-            counts[pr.fold] = ops.sample_counts(G, M) if pr.fold < 0 else fold_counts(G, M, seed, n_buckets, pr.fold)
-        pr.q_bat = counts[pr.fold]
+        if pr.fold not in shared:
+            Gf = G if pr.fold < 0 else fold_copy(G, M, seed, n_buckets, pr.fold)
+            shared[pr.fold] = (Gf, ops.sample_counts(Gf, M))
+        pr.G, pr.q_bat = shared[pr.fold]
 
 
-def _iteration(G, M, N, live, bmap):
+def _iteration(M, N, live):
     """One batched sweep over the live problems, then each one's targets + Adam move."""
-    batch = ops.EmBatch(M, N, [p.K for p in live], [p.fold for p in live], bmap, G.device)
-    batch.sweep(G, [p.P for p in live], [p.Q for p in live])
+    batch = ops.EmBatch(M, N, [p.K for p in live], live[0].G.device)
+    batch.sweep([p.G for p in live], [p.P for p in live], [p.Q for p in live])
     for k, pr in enumerate(live):
         pr.t += 1.0
         batch.adam(k, pr.P, pr.Q, pr.mP, pr.vP, pr.mQ, pr.vQ, pr.q_bat, pr.t, pr.lr, HP["beta1"], HP["beta2"],
@@ -103,18 +110,18 @@ def optimize_batch(G, M, N, problems, seed=0, n_buckets=10, max_iter=10000, chec
     A problem leaves the batch when it stops. ``fixed_iters=n``: every problem runs exactly
     n Adam-EM iterations (the first one from the start) and keeps its last iterate.
     Returns the problems (results in ``P_best``/``Q_best``)."""
+    problems = sorted(problems, key=lambda p: p.fold)   # problems on the same genotypes adjacent
     _prepare(G, M, problems, seed, n_buckets)
-    bmap = ops.cv_bucket_map(M, N, seed, n_buckets, G.device) if any(p.fold >= 0 for p in problems) else None
     if fixed_iters is not None:
         for _ in range(int(fixed_iters)):
-            _iteration(G, M, N, problems, bmap)
+            _iteration(M, N, problems)
         for pr in problems:
             pr.P_best, pr.Q_best = pr.P, pr.Q
         return problems
     if any(p.fold >= 0 for p in problems):
         raise ValueError("fold problems run a fixed number of iterations (fixed_iters)")
     # priming: one iteration, then the primed point's log-likelihood is the first best
-    _iteration(G, M, N, problems, bmap)
+    _iteration(M, N, problems)
     for pr in problems:
         pr.L_best = float(ops.loglik_device(G, pr.P, pr.Q, M, "f64").item())
         pr.P_best, pr.Q_best = pr.P.clone(), pr.Q.clone()
@@ -122,7 +129,7 @@ def optimize_batch(G, M, N, problems, seed=0, n_buckets=10, max_iter=10000, chec
         live = [p for p in problems if p.active]
         if not live:
             break
-        _iteration(G, M, N, live, bmap)
+        _iteration(M, N, live)
         if (it + 1) % check:
             continue
         for pr in live:
@@ -151,8 +158,7 @@ def _fit_alone(G, M, N, pr, max_iter, check, lr_decay, min_lr, patience, tol):
 
 
 def _polish_alone(G, M, N, P0, Q0, K, fold, seed, n_buckets, n_iters):
-    Gm = ops.masked_copy(G)
-    ops.cv_mask_hash(Gm, G, M, seed, n_buckets, fold)
+    Gm = fold_copy(G, M, seed, n_buckets, fold)
     P, Q = P0.clone(), Q0.clone()
     opt = EMAdamOptimizer(P.shape, Q.shape, HP["lr"], HP["beta1"], HP["beta2"], HP["eps"], G.device, "f64")
     ws = ops.Workspace.get(G.device, ops.em_workspace_bytes(M, N, K, "f64"))
@@ -191,7 +197,7 @@ def cross_validate(G, M, N, Ks, starts, n_folds=5, n_buckets=10, seed=42, polish
     torch.cuda.synchronize(dev)
     t1 = time.perf_counter()
     if batched:
-        probs = [Problem(K, *out["fits"][K], fold=f) for K in Ks for f in range(n_folds)]
+        probs = [Problem(K, *out["fits"][K], fold=f) for f in range(n_folds) for K in Ks]
         optimize_batch(G, M, N, probs, seed, n_buckets, fixed_iters=polish_iters)
         for pr in probs:
             out["folds"][(pr.K, pr.fold)] = (pr.P_best, pr.Q_best)

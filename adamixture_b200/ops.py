@@ -245,36 +245,32 @@ class EmBatch:
     """Host-side description of a batch of float64 E-step problems on one cohort (the
     C arrays the batch entry points take) and its partial-sum workspace."""
 
-    def __init__(self, M: int, N: int, Ks, folds, bucket_map: torch.Tensor | None = None, device=None):
+    def __init__(self, M: int, N: int, Ks, device=None):
         import ctypes
 
         self.M, self.N = int(M), int(N)
         self.n = len(Ks)
         self.K = (ctypes.c_int * self.n)(*[int(k) for k in Ks])
-        self.fold = (ctypes.c_int * self.n)(*[int(f) for f in folds])
-        if any(int(f) >= 0 for f in folds):
-            if bucket_map is None or bucket_map.shape != (self.M, self.N) or bucket_map.dtype != torch.uint8:
-                raise ValueError("fold problems need the [M, N] uint8 bucket map (cv_bucket_map)")
-        self.bucket_map = bucket_map
         nbytes = query_size("adx_em_batch_workspace_bytes", self.M, self.N, self.n, ctypes.addressof(self.K))
         dev = torch.device("cuda", torch.cuda.current_device()) if device is None else torch.device(device)
         self.workspace = Workspace.get(dev, nbytes, tag="em_batch")
 
-    def sweep(self, G: torch.Tensor, Ps, Qs) -> None:
-        """One batched sweep over the problems (P, Q: float64 device tensors)."""
+    def sweep(self, Gs, Ps, Qs) -> None:
+        """One batched sweep: problem p on packed genotypes Gs[p] with Ps[p], Qs[p] (float64)."""
         import ctypes
 
-        _check(G, "G", torch.uint8)
-        for P, Q, k in zip(Ps, Qs, self.K):
+        for G, P, Q, k in zip(Gs, Ps, Qs, self.K):
+            _check(G, "G", torch.uint8)
             _check(P, "P", torch.float64, G.device)
             _check(Q, "Q", torch.float64, G.device)
-            if P.shape != (self.M, k) or Q.shape != (self.N, k):
-                raise ValueError("P/Q shapes do not match the batch")
+            if P.shape != (self.M, k) or Q.shape != (self.N, k) or G.shape != ((self.M + 3) // 4, self.N):
+                raise ValueError("G/P/Q shapes do not match the batch")
+        gg = (ctypes.c_void_p * self.n)(*[G.data_ptr() for G in Gs])
         pp = (ctypes.c_void_p * self.n)(*[P.data_ptr() for P in Ps])
         qq = (ctypes.c_void_p * self.n)(*[Q.data_ptr() for Q in Qs])
-        call("adx_em_sweep_batch", G.data_ptr(), self.M, self.N, self.n, ctypes.addressof(self.K),
-             ctypes.addressof(self.fold), _ptr(self.bucket_map), ctypes.addressof(pp), ctypes.addressof(qq),
-             self.workspace.data_ptr(), self.workspace.numel(), _stream(G.device))
+        call("adx_em_sweep_batch", self.M, self.N, self.n, ctypes.addressof(self.K), ctypes.addressof(gg),
+             ctypes.addressof(pp), ctypes.addressof(qq), self.workspace.data_ptr(), self.workspace.numel(),
+             _stream(Gs[0].device))
 
     def stats(self, p: int):
         """A, B, T of problem p from the last sweep."""
@@ -298,14 +294,6 @@ class EmBatch:
              q_bat.data_ptr(), P.data_ptr(), Q.data_ptr(), mP.data_ptr(), vP.data_ptr(), mQ.data_ptr(),
              vQ.data_ptr(), float(t), float(lr), float(beta1), float(beta2), float(eps),
              self.workspace.data_ptr(), self.workspace.numel(), _stream(P.device))
-
-
-def cv_bucket_map(M: int, N: int, seed: int, n_buckets: int, device=None) -> torch.Tensor:
-    """[M, N] uint8: the hash fold rule's bucket of every entry."""
-    dev = torch.device("cuda", torch.cuda.current_device()) if device is None else torch.device(device)
-    out = torch.empty((M, N), dtype=torch.uint8, device=dev)
-    call("adx_cv_bucket_map", M, N, int(seed) & 0xFFFFFFFFFFFFFFFF, int(n_buckets), out.data_ptr(), _stream(dev))
-    return out
 
 
 def loglik_device(G: torch.Tensor, P: torch.Tensor, Q: torch.Tensor, M: int, precision="f64",

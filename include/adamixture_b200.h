@@ -146,18 +146,19 @@ int adx_em_adam_iteration(const uint8_t* G, int64_t M, int64_t N, int K, int pre
 
 /* ---------------------------------------------------------------- batched float64 E-step
  * Several Adam-EM problems on one cohort in one sweep launch: n <= 64 problems, each with its
- * own K[p] <= 16, P[p] [M][K[p]] and Q[p] [N][K[p]] (device float64; the arrays of pointers
- * and K/fold are HOST arrays), and a fold: entries whose bucket in `bucket_map` equals
- * fold[p] are treated as missing (fold[p] = -1: none; bucket_map may be NULL when no problem
- * has a fold). Each CTA reads a genotype tile once and runs every problem on it. Every
- * problem's statistics are bit-identical to the single-problem float64 sweep (adx_em_stats /
- * adx_em_adam_iteration at ADX_F64) of the same P, Q and masked genotypes. The reference runs
- * the K sweep and its CV folds one after the other (adamixture/src/main.py:67-107,
+ * own packed genotypes G[p] (the same matrix, or for a cross-validation fold a copy with the
+ * fold's entries hidden, e.g. by adx_cv_mask_hash), K[p] <= 16, P[p] [M][K[p]] and Q[p]
+ * [N][K[p]] (device pointers, float64; the arrays of pointers and K are HOST arrays). Each
+ * CTA runs the problems in order over its share of the matrix, so consecutive problems on
+ * the same genotypes read them from memory once (from L2 after the first). Every problem's
+ * statistics are bit-identical to the single-problem float64 sweep (adx_em_stats /
+ * adx_em_adam_iteration at ADX_F64) of the same G, P and Q. The reference runs the K sweep
+ * and its CV folds one after the other (adamixture/src/main.py:67-107,
  * adamixture/src/cv.py:171-267); no counterpart batches them. */
 int adx_em_batch_workspace_bytes(int64_t M, int64_t N, int n, const int* K, size_t* bytes);
-int adx_em_sweep_batch(const uint8_t* G, int64_t M, int64_t N, int n, const int* K, const int* fold,
-                       const uint8_t* bucket_map, const double* const* P, const double* const* Q,
-                       void* workspace, size_t workspace_bytes, void* stream);
+int adx_em_sweep_batch(int64_t M, int64_t N, int n, const int* K, const uint8_t* const* G,
+                       const double* const* P, const double* const* Q, void* workspace,
+                       size_t workspace_bytes, void* stream);
 /* Problem p of the last batched sweep in `workspace`: mode 0 writes its A, B, T (float64);
  * mode 1 forms the EM targets and applies the Adam move to its P, Q and moments (t = step
  * count after the increment), as adx_em_adam_iteration does. */
@@ -250,10 +251,6 @@ int adx_cv_mask_hash(uint8_t* G, size_t g_bytes, const uint8_t* G0, int64_t M, i
 int adx_cv_deviance_list(const uint8_t* G0, int64_t M, int64_t N, int K, const double* P,
                          const double* Q, const int64_t* idx, int64_t n, double* out,
                          void* workspace, size_t workspace_bytes, void* stream);
-/* map[j*N + i] = h(j*N + i, seed) mod n_buckets (uint8 [M][N], 1 <= n_buckets <= 255): the
- * reference's hash fold rule (cv.py:58-78) evaluated once for every entry, for
- * adx_em_sweep_batch. With n_buckets = 10, bucket f (f < 5) holds 10 % of the entries. */
-int adx_cv_bucket_map(int64_t M, int64_t N, uint64_t seed, int n_buckets, uint8_t* map, void* stream);
 int adx_cv_deviance_hash(const uint8_t* G0, int64_t M, int64_t N, int K, const double* P,
                          const double* Q, uint64_t seed, int n_folds, int fold, double* out,
                          void* workspace, size_t workspace_bytes, void* stream);

@@ -39,24 +39,23 @@ def _start(M, N, K, seed):
 
 @pytest.mark.parametrize("N,M", [(1000, 777), (2048, 301)])
 def test_batched_stats_equal_single_problem_sweeps(ops, N, M):
+    from adamixture_b200.model.em_adam_batch import fold_copy
+
     G = _cohort(N, M, 4, N + M)
     Ks = [2, 5, 10, 16, 3, 12]
     folds = [-1, 0, 3, -1, 9, 4]
     seed = 42
     starts = [_start(M, N, K, 10 + i) for i, K in enumerate(Ks)]
-    batch = ops.EmBatch(M, N, Ks, folds, ops.cv_bucket_map(M, N, seed, 10), G.device)
-    batch.sweep(G, [s[0] for s in starts], [s[1] for s in starts])
+    Gs = [G if f < 0 else fold_copy(G, M, seed, 10, f) for f in folds]
+    batch = ops.EmBatch(M, N, Ks, G.device)
+    batch.sweep(Gs, [s[0] for s in starts], [s[1] for s in starts])
     for p, (K, f) in enumerate(zip(Ks, folds)):
         A, B, T = batch.stats(p)
-        Gp = G
-        if f >= 0:
-            Gp = ops.masked_copy(G)
-            ops.cv_mask_hash(Gp, G, M, seed, 10, f)
-        A1, B1, T1 = ops.em_stats(Gp, starts[p][0], starts[p][1], M, "f64")
+        A1, B1, T1 = ops.em_stats(Gs[p], starts[p][0], starts[p][1], M, "f64")
         for got, ref in ((A, A1), (B, B1), (T, T1)):
             assert torch.equal(got, ref), (K, f, float((got - ref).abs().max()))
         # and against the float64 oracle on the masked genotypes
-        Gu = orc.unpack(Gp.cpu().numpy(), M)
+        Gu = orc.unpack(Gs[p].cpu().numpy(), M)
         A0, B0, T0, _ = orc.em_stats(Gu, starts[p][0].cpu().numpy(), starts[p][1].cpu().numpy())
         for got, ref in ((A, A0), (B, B0), (T, T0)):
             err = np.abs(got.cpu().numpy() - ref).max() / np.abs(ref).max()
