@@ -123,17 +123,13 @@ struct Probs {
   int n;
 };
 
-// KS: k-steps of 4 covering every problem's K (K <= 4 KS); NK = ceil(KS / 2) column tiles
-// of 8 (registers are sized by them; a batch skips each problem's k-steps and column tiles
-// beyond its own K, which only ever add exact zeros). A CTA runs the problems in order,
-// each over the CTA's whole share of the matrix (its SNP block x its sample sub-tiles), so
-// consecutive problems on the same genotypes find the CTA's genotype region (about 0.3 MB
-// at N=20k, M=100k) still in L2 and read it from memory once; a problem's arithmetic and
-// summation order do not depend on the other problems.
-template <int KS, int MAXP>
-__global__ void __launch_bounds__(TPB, 1) em_sweep_dmma_kernel(Args a, Probs<MAXP> ps) {
+// KS: k-steps of 4 covering the problem's K (K <= 4 KS); NK = ceil(KS / 2) column tiles of
+// 8. One (problem, sample sub-tile) of a CTA: the sub-tile's Q rows, then the CTA's SNP
+// block in groups of 8 chunks of 16 SNPs, then the sub-tile's T partials.
+template <int KS>
+__device__ __forceinline__ void sweep_subtile(const Args& a, const Prob& pr, int64_t st, int split, int mblk,
+                                              int& chunk_no, double* sm) {
   constexpr int NK = (KS + 1) / 2;
-  extern __shared__ __align__(16) double sm[];
   double* qt = sm + Q_OFF;   // [W][QSTR]: Q rows of the sub-tile, columns swizzled by qsw(row)
   double* pt = sm + P_OFF;   // [GS][PSTR]: P rows of the group
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -141,19 +137,11 @@ __global__ void __launch_bounds__(TPB, 1) em_sweep_dmma_kernel(Args a, Probs<MAX
   double* dT = sm + D_OFF + warp * WS * DSTR;  // [WS][DSTR]: d^T of the warp's tile
   double* sbuf = sm + S_OFF + warp * WS;
   const int64_t N = a.N, M = a.M;
-  const int mblk = blockIdx.x % a.n_mblk;
-  const int split = blockIdx.x / a.n_mblk;
   const int64_t j0 = (int64_t)mblk * a.mb;
   const int64_t j1 = min(M, j0 + a.mb);
   const int64_t rows = (M + 3) >> 2;
-  int chunk_no = 0;   // parity of the A/B reduction buffer
-
-  for (int pi = 0; pi < (MAXP == 1 ? 1 : ps.n); ++pi)
-  for (int64_t st = split; st < a.n_stile; st += a.n_split) {
-    const Prob pr = ps.p[pi];
     const int K = pr.K;
-    const int ksp = MAXP == 1 ? KS : (K + 3) >> 2;   // this problem's k-steps and column tiles
-    const int nkp = MAXP == 1 ? NK : (ksp + 1) >> 1;
+    constexpr int ksp = KS, nkp = NK;
     const bool first = st == split;   // this CTA's first sub-tile: AB_part rows are written
     const int64_t i0 = st * W;
     // Q rows of the sub-tile (zero beyond N and K); the previous sub-tile's last reads of
@@ -375,6 +363,34 @@ __global__ void __launch_bounds__(TPB, 1) em_sweep_dmma_kernel(Args a, Probs<MAX
     __syncwarp();
     // qt is rewritten at the next (sub-tile, problem)'s start: every warp's reads of it precede the
     // last chunk barrier, which all threads have passed
+}
+
+// A single problem (MAXP = 1, KS its own) or a batch of up to MAXP problems (each run by the
+// instance of its own K). A CTA runs the problems in order, each over the CTA's whole share
+// of the matrix (its SNP block x its sample sub-tiles), so consecutive problems on the same
+// genotypes find the CTA's genotype region (about 0.3 MB at N=20k, M=100k) still in L2 and
+// read it from memory once; a problem's arithmetic and summation order do not depend on the
+// other problems.
+template <int KS, int MAXP>
+__global__ void __launch_bounds__(TPB, 1) em_sweep_dmma_kernel(Args a, Probs<MAXP> ps) {
+  extern __shared__ __align__(16) double sm[];
+  const int mblk = blockIdx.x % a.n_mblk;
+  const int split = blockIdx.x / a.n_mblk;
+  int chunk_no = 0;   // parity of the A/B reduction buffer
+  for (int pi = 0; pi < (MAXP == 1 ? 1 : ps.n); ++pi) {
+    const Prob pr = ps.p[pi];
+    for (int64_t st = split; st < a.n_stile; st += a.n_split) {
+      if constexpr (MAXP == 1) {
+        sweep_subtile<KS>(a, pr, st, split, mblk, chunk_no, sm);
+      } else {
+        switch ((pr.K + 3) >> 2) {
+          case 1: sweep_subtile<1>(a, pr, st, split, mblk, chunk_no, sm); break;
+          case 2: sweep_subtile<2>(a, pr, st, split, mblk, chunk_no, sm); break;
+          case 3: sweep_subtile<3>(a, pr, st, split, mblk, chunk_no, sm); break;
+          default: sweep_subtile<4>(a, pr, st, split, mblk, chunk_no, sm); break;
+        }
+      }
+    }
   }
 }
 
@@ -426,19 +442,12 @@ int dmma_sweep_batch(int64_t M, int64_t N, int n, const int* K, const uint8_t* c
   if (n < 1 || n > DMMA_MAX_PROBLEMS) return ADX_ERR_ARG;
   const dm::Args a{M, N, n_stile, n_split, n_mblk, mb};
   dm::Probs<DMMA_MAX_PROBLEMS> ps;
-  int kmax = 1;
   for (int p = 0; p < n; ++p) {
     if (K[p] < 1 || K[p] > 16 || !G[p]) return ADX_ERR_ARG;
     ps.p[p] = dm::Prob{G[p], P[p], Q[p], ABp[p], Tp[p], K[p], dmma_vec(G[p], N)};
-    kmax = K[p] > kmax ? K[p] : kmax;
   }
   ps.n = n;
-  switch ((kmax + 3) / 4) {
-    case 1: return dmma_launch<1, DMMA_MAX_PROBLEMS>(a, ps, st);
-    case 2: return dmma_launch<2, DMMA_MAX_PROBLEMS>(a, ps, st);
-    case 3: return dmma_launch<3, DMMA_MAX_PROBLEMS>(a, ps, st);
-    default: return dmma_launch<4, DMMA_MAX_PROBLEMS>(a, ps, st);
-  }
+  return dmma_launch<4, DMMA_MAX_PROBLEMS>(a, ps, st);
 }
 
 }  // namespace adx
