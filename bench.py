@@ -855,6 +855,42 @@ def run_errors(args, cfg):
         "loglik": "float64 log-likelihood of each run's own P, Q"}, "runs": out}), flush=True)
 
 
+def run_batch_sweeps(G, M, N, Ks, starts, dev):
+    """``--config c4 --batch-sweeps``: one float64 sweep launch per K alone, the batched
+    entry point with that one problem, all K in one batched launch, and all K on fold 0's
+    masked copy (CUDA events, mean of 5 launches after one warm-up; 3 for the batches)."""
+    import torch
+
+    from adamixture_b200 import ops
+    from adamixture_b200.model.em_adam_batch import fold_copy
+
+    def timed(fn, reps=5):
+        fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    out = {}
+    for K in Ks:
+        ws = ops.Workspace.get(dev, ops.em_workspace_bytes(M, N, K, "f64"))
+        out[f"single_K{K}"] = timed(lambda: ops.em_sweep(G, starts[K][0], starts[K][1], M, "f64", ws))
+        b1 = ops.EmBatch(M, N, [K], dev)
+        out[f"batch1_K{K}"] = timed(lambda: b1.sweep([G], [starts[K][0]], [starts[K][1]]))
+    b = ops.EmBatch(M, N, Ks, dev)
+    out["batch_all"] = timed(lambda: b.sweep([G] * len(Ks), [starts[K][0] for K in Ks], [starts[K][1] for K in Ks]), 3)
+    out["sum_single"] = sum(out[f"single_K{K}"] for K in Ks)
+    Gf = fold_copy(G, M, 42, 10, 0)
+    out["batch_fold0_all"] = timed(lambda: b.sweep([Gf] * len(Ks), [starts[K][0] for K in Ks],
+                                                   [starts[K][1] for K in Ks]), 3)
+    print(json.dumps({"metric": "float64 sweep launch ms, single vs batched", "N": N, "M": M, "ms": out}),
+          flush=True)
+
+
 def run_cv_batch(args, cfg):
     """``--config c4``: the K sweep K=2..12 and 5-fold cross-validation (10 % of the
     entries per fold by the seeded hash rule) as batched problems -- every iteration one
@@ -880,6 +916,9 @@ def run_cv_batch(args, cfg):
         Q0 = np.clip(rng.random((N, K)), 1e-5, 1 - 1e-5)
         Q0 /= Q0.sum(1, keepdims=True)
         starts[K] = (torch.from_numpy(P0).to(dev), torch.from_numpy(Q0).to(dev))
+    if args.batch_sweeps:
+        run_batch_sweeps(G, M, N, Ks, starts, dev)
+        return
     kw = dict(n_folds=5, n_buckets=10, seed=42, polish_iters=args.cv_polish, max_iter=args.cv_max_iter)
     # load the kernel instances both paths use before timing
     cross_validate(G, M, N, [2, 12], starts, **{**kw, "max_iter": 5, "polish_iters": 1}, batched=True)
@@ -971,6 +1010,8 @@ def main():
                     help="c4: iteration cap of the full-data fits")
     ap.add_argument("--cv-polish", dest="cv_polish", type=int, default=10,
                     help="c4: Adam-EM iterations per fold")
+    ap.add_argument("--batch-sweeps", dest="batch_sweeps", action="store_true",
+                    help="c4: time single and batched sweep launches instead of the CV runs")
     ap.add_argument("--kernels-skip-hessian", dest="kernels_skip_hessian", action="store_true")
     ap.add_argument("--sweep-by-k", dest="sweep_by_k", action="store_true",
                     help="float32 vs FP16 tensor-core sweep time for K = 2..16")
