@@ -683,6 +683,22 @@ extern "C" int adx_em_adam_iteration(const uint8_t* G, int64_t M, int64_t N, int
                    vQ, AdamArgs{t, lr, beta1, beta2, eps}, st);
 }
 
+// The float64 log-likelihood on the float64 MMA (em_sweep_dmma.cu) uses the float64 sweep's
+// partition; ADX_ERR_UNSUPPORTED when K > 16.
+namespace adx {
+int dmma_loglik_plan(int64_t M, int64_t N, int K, int64_t& n_stile, int& n_split, int& n_mblk, int64_t& mb) {
+  if (K > DMMA_MAX_K) return ADX_ERR_UNSUPPORTED;
+  EmPlan pl;
+  const int rc = em_plan(M, N, K, ADX_F64, pl);
+  if (rc) return rc;
+  n_stile = pl.n_stile;
+  n_split = pl.n_split;
+  n_mblk = pl.n_mblk;
+  mb = pl.mb;
+  return ADX_OK;
+}
+}  // namespace adx
+
 // ---------------------------------------------------------------- batched float64 E-step
 //
 // Several E-step problems on one cohort (K <= 16 each; e.g. the K sweep and its cross-

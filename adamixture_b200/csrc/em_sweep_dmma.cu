@@ -394,6 +394,125 @@ __global__ void __launch_bounds__(TPB, 1) em_sweep_dmma_kernel(Args a, Probs<MAX
   }
 }
 
+// ---------------------------------------------------------------- float64 log-likelihood
+//
+// The log-likelihood of (P, Q) (adamixture/model/em_adam_gpu.py:226-279) with h on the same
+// float64 MMA tiles as the sweep: L = sum over observed (j, i) of g log h + (2-g) log(1-h),
+// h = clamp(P_j . Q_i, 1e-10, 1-1e-10). As in loglik_kernel, each thread multiplies the
+// per-entry factors h^g (1-h)^(2-g) (the product x*y of two values picked by the genotype's
+// two bits; 1 when missing) into one float64 running product, moves its exponent into an
+// integer after every 4 factors (>= 1e-80 together, so the product stays normal), and takes
+// one log at the end; per-CTA sums in a fixed order, per-CTA partials summed in block order.
+
+__device__ __forceinline__ double renorm_dm(double x, int& e) {
+  int hi = __double2hiint(x);
+  const int lo = __double2loint(x);
+  e += ((hi >> 20) & 0x7FF) - 1022;
+  hi = (hi & 0x800FFFFF) | (1022 << 20);
+  return __hiloint2double(hi, lo);
+}
+
+// shared memory of the log-likelihood: the Q and P tiles and the warp sums (doubles)
+constexpr int LL_SMEM_DOUBLES = P_OFF + GS * PSTR + WARPS;
+constexpr size_t LL_SMEM_BYTES = sizeof(double) * LL_SMEM_DOUBLES;
+
+template <int KS>
+__global__ void __launch_bounds__(TPB, 2) loglik_dmma_kernel(Args a, const uint8_t* __restrict__ G,
+                                                             const double* __restrict__ P,
+                                                             const double* __restrict__ Q, int K, int vec,
+                                                             double* __restrict__ partial) {
+  extern __shared__ __align__(16) double sm[];
+  double* qt = sm + Q_OFF;
+  double* pt = sm + P_OFF;
+  double* wsum = sm + P_OFF + GS * PSTR;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int g = lane >> 2, t = lane & 3;
+  const int64_t N = a.N, M = a.M;
+  const int mblk = blockIdx.x % a.n_mblk;
+  const int split = blockIdx.x / a.n_mblk;
+  const int64_t j0 = (int64_t)mblk * a.mb;
+  const int64_t j1 = min(M, j0 + a.mb);
+  const int64_t rows = (M + 3) >> 2;
+  double prod = 1.0;
+  int ex = 0;
+  for (int64_t st = split; st < a.n_stile; st += a.n_split) {
+    const int64_t i0 = st * W;
+    __syncthreads();   // the previous sub-tile's reads of qt and pt are done
+    for (int e = threadIdx.x; e < W * 16; e += TPB) {
+      const int r = e >> 4, k = e & 15;
+      const int64_t i = i0 + r;
+      qt[r * QSTR + (k ^ qsw(r))] = (i < N && k < K) ? Q[i * K + k] : 0.0;
+    }
+    const int64_t s0 = i0 + warp * WS + 8 * t;
+    const bool full8 = vec && (s0 + 8 <= N);
+    uint64_t wnext[2];
+    load_words(G, N, rows, j0, g, s0, full8, wnext);
+    for (int64_t gj = j0; gj < j1; gj += GS) {
+      const int gn = (int)min((int64_t)GS, j1 - gj);
+      __syncthreads();
+      for (int e = threadIdx.x; e < GS * 16; e += TPB) {
+        const int r = e >> 4, k = e & 15;
+        pt[r * PSTR + k] = (r < gn && k < K) ? P[(gj + r) * K + k] : 0.0;
+      }
+      __syncthreads();
+      const int nch = (gn + CH - 1) / CH;
+      for (int ch = 0; ch < nch; ++ch) {
+        const int64_t jc = gj + ch * CH;
+        const double* pc = pt + ch * CH * PSTR;
+        uint64_t w[2] = {wnext[0], wnext[1]};
+        if (jc + CH < j1) load_words(G, N, rows, jc + CH, g, s0, full8, wnext);
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          if (jc + g + 8 * h >= j1) w[h] |= 0x0303030303030303ull << (2 * (g & 3));
+          w[h] >>= 2 * (g & 3);
+        }
+        double ph[KS][2];
+#pragma unroll
+        for (int ks = 0; ks < KS; ++ks) {
+          ph[ks][0] = pc[g * PSTR + 4 * ks + t];
+          ph[ks][1] = pc[(g + 8) * PSTR + 4 * ks + t];
+        }
+        double hacc[4][4];
+#pragma unroll
+        for (int nt = 0; nt < 4; ++nt) {
+          const int qrow = warp * WS + 8 * (g >> 1) + 2 * nt + (g & 1);
+          hacc[nt][0] = hacc[nt][1] = hacc[nt][2] = hacc[nt][3] = 0.0;
+#pragma unroll
+          for (int ks = 0; ks < KS; ++ks)
+            mma_f64(hacc[nt], ph[ks][0], ph[ks][1], qt[qrow * QSTR + ((4 * ks + t) ^ qsw(qrow))]);
+        }
+#pragma unroll
+        for (int nt = 0; nt < 4; ++nt) {
+          double f[4];
+#pragma unroll
+          for (int e = 0; e < 4; ++e) {
+            const uint32_t code = (uint32_t)(w[e >> 1] >> (8 * (2 * nt + (e & 1)))) & 3u;
+            const double h = fmin(fmax(hacc[nt][e], LL_CLAMP), 1.0 - LL_CLAMP);
+            const double om = 1.0 - h;
+            const double x = code == 2u ? h : om;
+            const double y = code == 0u ? om : h;
+            f[e] = code == 3u ? 1.0 : x * y;
+          }
+          prod *= (f[0] * f[1]) * (f[2] * f[3]);
+          prod = renorm_dm(prod, ex);
+        }
+      }
+    }
+  }
+  double acc = log(prod) + (double)ex * 0.69314718055994530942;
+  // fixed-order block sum: warps by shuffles, then the 8 warp sums in order
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  __syncthreads();
+  if (lane == 0) wsum[warp] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s = 0.0;
+    for (int w2 = 0; w2 < WARPS; ++w2) s += wsum[w2];
+    partial[blockIdx.x] = s;
+  }
+}
+
 }  // namespace dm
 
 int dmma_plan_width() { return dm::W; }
@@ -448,6 +567,49 @@ int dmma_sweep_batch(int64_t M, int64_t N, int n, const int* K, const uint8_t* c
   }
   ps.n = n;
   return dmma_launch<4, DMMA_MAX_PROBLEMS>(a, ps, st);
+}
+
+}  // namespace adx
+
+namespace adx {
+
+// Float64 log-likelihood on the float64 MMA for K <= 16: the float64 sweep's partition
+// (n_split x n_mblk CTAs, at most 1776), one partial per CTA. Returns the partial count
+// through *nblk (0 when this form does not apply).
+int dmma_loglik_plan(int64_t M, int64_t N, int K, int64_t& n_stile, int& n_split, int& n_mblk, int64_t& mb);
+
+int dmma_loglik(const uint8_t* G, const double* P, const double* Q, int64_t M, int64_t N, int K, double* partial,
+                int* nblk, cudaStream_t st) {
+  int64_t n_stile = 0, mb = 0;
+  int n_split = 0, n_mblk = 0;
+  int rc = dmma_loglik_plan(M, N, K, n_stile, n_split, n_mblk, mb);
+  if (rc) return rc;
+  *nblk = n_split * n_mblk;
+  if (!partial) return ADX_OK;
+  const dm::Args a{M, N, n_stile, n_split, n_mblk, mb};
+  const int vec = dmma_vec(G, N);
+#define ADX_LL_DM(KS)                                                                                          \
+  {                                                                                                            \
+    static bool attr_set[64] = {false};                                                                        \
+    int dev = 0;                                                                                               \
+    ADX_CUDA_TRY(cudaGetDevice(&dev));                                                                         \
+    if (dev >= 0 && dev < 64 && !attr_set[dev]) {                                                              \
+      ADX_CUDA_TRY(cudaFuncSetAttribute(dm::loglik_dmma_kernel<KS>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
+                                        (int)dm::LL_SMEM_BYTES));                                              \
+      attr_set[dev] = true;                                                                                    \
+    }                                                                                                          \
+    dm::loglik_dmma_kernel<KS><<<(unsigned)(n_split * n_mblk), dm::TPB, dm::LL_SMEM_BYTES, st>>>(a, G, P, Q, K,  \
+                                                                                              vec, partial);   \
+  }
+  switch ((K + 3) / 4) {
+    case 1: ADX_LL_DM(1) break;
+    case 2: ADX_LL_DM(2) break;
+    case 3: ADX_LL_DM(3) break;
+    default: ADX_LL_DM(4) break;
+  }
+#undef ADX_LL_DM
+  ADX_LAUNCH_CHECK();
+  return ADX_OK;
 }
 
 }  // namespace adx

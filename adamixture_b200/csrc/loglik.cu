@@ -286,11 +286,22 @@ static int ll_plan(int64_t M, int64_t N, int K, int prec, LlPlan& pl) {
 
 using namespace adx;
 
+// Float64 with K <= 16: h on the float64 MMA tiles of the float64 sweep (em_sweep_dmma.cu);
+// `nblk` receives its partial count, and partial == nullptr only queries it.
+int dmma_loglik(const uint8_t* G, const double* P, const double* Q, int64_t M, int64_t N, int K, double* partial,
+                int* nblk, cudaStream_t st);
+constexpr int LL_DMMA_MAX_K = 16;
+
 extern "C" int adx_loglik_workspace_bytes(int64_t M, int64_t N, int K, int precision, size_t* bytes) {
   LlPlan pl;
   const int rc = ll_plan(M, N, K, precision, pl);
   if (rc || !bytes) { adx_set_message("adx_loglik_workspace_bytes: bad arguments"); return rc ? rc : ADX_ERR_ARG; }
-  *bytes = (size_t)pl.n_split * pl.n_mblk * sizeof(double) + 256;
+  int nblk = pl.n_split * pl.n_mblk;
+  if (precision == ADX_F64 && K <= LL_DMMA_MAX_K) {
+    int nd = 0;
+    if (dmma_loglik(nullptr, nullptr, nullptr, M, N, K, nullptr, &nd, nullptr) == ADX_OK && nd > nblk) nblk = nd;
+  }
+  *bytes = (size_t)nblk * sizeof(double) + 256;
   return ADX_OK;
 }
 
@@ -301,10 +312,21 @@ extern "C" int adx_loglik(const uint8_t* G, int64_t M, int64_t N, int K, int pre
   int rc = ll_plan(M, N, K, precision, pl);
   if (rc) { adx_set_message("adx_loglik: bad shape or precision"); return rc; }
   if (!G || !P || !Q || !out || !workspace) { adx_set_message("adx_loglik: null pointer"); return ADX_ERR_ARG; }
-  const int nblk = pl.n_split * pl.n_mblk;
-  if (workspace_bytes < (size_t)nblk * sizeof(double)) { adx_set_message("adx_loglik: workspace too small"); return ADX_ERR_WORKSPACE; }
   double* part = reinterpret_cast<double*>(workspace);
   cudaStream_t st = as_stream(stream);
+  if (precision == ADX_F64 && K <= LL_DMMA_MAX_K) {
+    int nd = 0;
+    rc = dmma_loglik(G, (const double*)P, (const double*)Q, M, N, K, nullptr, &nd, st);
+    if (rc) return rc;
+    if (workspace_bytes < (size_t)nd * sizeof(double)) { adx_set_message("adx_loglik: workspace too small"); return ADX_ERR_WORKSPACE; }
+    rc = dmma_loglik(G, (const double*)P, (const double*)Q, M, N, K, part, &nd, st);
+    if (rc) return rc;
+    sum_partials_kernel<<<1, 256, 0, st>>>(part, nd, out);
+    ADX_LAUNCH_CHECK();
+    return ADX_OK;
+  }
+  const int nblk = pl.n_split * pl.n_mblk;
+  if (workspace_bytes < (size_t)nblk * sizeof(double)) { adx_set_message("adx_loglik: workspace too small"); return ADX_ERR_WORKSPACE; }
   const int vec = ll_vec_loads(G, N, pl.spt);
 #define L64(KM) loglik_kernel<double, KM><<<nblk, LL_TPB, 0, st>>>(G, (const double*)P, (const double*)Q, M, N, K, pl.n_stile, pl.n_split, pl.n_mblk, pl.mb, vec, part)
 #define L32(KM) loglik_kernel<float, KM><<<nblk, LL_TPB, 0, st>>>(G, (const float*)P, (const float*)Q, M, N, K, pl.n_stile, pl.n_split, pl.n_mblk, pl.mb, vec, part)
@@ -383,6 +405,18 @@ extern "C" int adx_loglik_noalloc(const uint8_t* G, int64_t M, int64_t N, int K,
   rc = ll_noalloc_scratch(&part);
   if (rc) return rc;
   cudaStream_t st = as_stream(stream);
+  if (precision == ADX_F64 && K <= LL_DMMA_MAX_K) {
+    // the float64 MMA form, as adx_loglik runs it (at most 1776 partials)
+    int nd = 0;
+    rc = dmma_loglik(G, (const double*)P, (const double*)Q, M, N, K, nullptr, &nd, st);
+    if (rc) return rc;
+    if (nd > ADX_LL_NOALLOC_MAX_PARTIALS) { adx_set_message("adx_loglik_noalloc: plan too large"); return ADX_ERR_WORKSPACE; }
+    rc = dmma_loglik(G, (const double*)P, (const double*)Q, M, N, K, part, &nd, st);
+    if (rc) return rc;
+    sum_partials_kernel<<<1, 256, 0, st>>>(part, nd, out);
+    ADX_LAUNCH_CHECK();
+    return ADX_OK;
+  }
   const int vec = ll_vec_loads(G, N, pl.spt);
 #define N64(KM) loglik_kernel<double, KM><<<nblk, LL_TPB, 0, st>>>(G, (const double*)P, (const double*)Q, M, N, K, pl.n_stile, pl.n_split, pl.n_mblk, pl.mb, vec, part)
 #define N32(KM) loglik_kernel<float, KM><<<nblk, LL_TPB, 0, st>>>(G, (const float*)P, (const float*)Q, M, N, K, pl.n_stile, pl.n_split, pl.n_mblk, pl.mb, vec, part)

@@ -304,13 +304,27 @@ def warm_start_fit(net: WarmStartMLP, G, N: int, M: int, K: int, seed: int = 42,
     t_plain = time.perf_counter() - t0 + t_init
     t0 = time.perf_counter()
     P_w0, Q_w0 = predict(net, G, M, U, S, V, Q_als, P_als)
+    torch.cuda.synchronize()
+    t_pred = time.perf_counter() - t0
     P_w, Q_w, L_w, tr_w = run_em(G, N, M, K, P_w0, Q_w0, precision)
     torch.cuda.synchronize()
     t_warm = time.perf_counter() - t0 + t_init
     keep = L_w >= L_p - 1e-6 * abs(L_p)
+    target = max(e[1] for e in tr_p) if tr_p else None
+
+    def seconds_to(trace, extra):
+        for it, L, sec in trace:
+            if L >= target - 1e-6 * abs(target):
+                return sec + extra
+        return None
+
     return {
         "loglik_plain": L_p, "loglik_warm": L_w, "kept_warm": bool(keep),
-        "seconds_plain": t_plain, "seconds_warm": t_warm,
+        "seconds_plain": t_plain, "seconds_warm": t_warm, "seconds_init": t_init, "seconds_predict": t_pred,
+        # wall time from the start of initialisation to the first check within 1e-6 of the
+        # plain run's converged log-likelihood
+        "seconds_to_target_plain": seconds_to(tr_p, t_init) if tr_p else None,
+        "seconds_to_target_warm": seconds_to(tr_w, t_init + t_pred) if tr_p else None,
         # traced values share the runs' log-likelihood arithmetic: compare within it
         "iters_plain": iterations_to_reach(tr_p, max(e[1] for e in tr_p)) if tr_p else None,
         "iters_warm_to_plain": iterations_to_reach(tr_w, max(e[1] for e in tr_p)) if tr_p else None,

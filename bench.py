@@ -60,6 +60,8 @@ CONFIGS = {
                N=1_000, M=10_000, K=3, F=0.1, alpha=0.5, miss=0.01, seed=0),
     "c4": dict(workload="K sweep K=2..12 with 5-fold CV (10 % of entries per fold, seeded hash), N=20000 samples, M=100000 SNPs, true K=6, F=0.08, Q Dir(0.5), 1% missing",
                N=20_000, M=100_000, K=6, F=0.08, alpha=0.5, miss=0.01, seed=4000),
+    "c5": dict(workload="learned warm start vs the ALS start, held-out cohort N=100000 samples, M=300000 SNPs, K=8, F=0.05, Q Dir(0.5), 1% missing",
+               N=100_000, M=300_000, K=8, F=0.05, alpha=0.5, miss=0.01, seed=5000),
     # the c3 cohort's generator at one tenth of its SNPs (2.5 GB packed): the size profiled
     # under ncu, whose full capture saves and restores device memory on every pass
     "c3s": dict(workload="Adam-EM, N=200000 samples, M=50000 SNPs, K=10, F=0.02, Q 0.7*Dir(0.05)+0.3*Dir(1), 1% missing",
@@ -946,6 +948,41 @@ def run_cv_batch(args, cfg):
     print(json.dumps(line), flush=True)
 
 
+def run_warm_start(args, cfg):
+    """``--config c5``: the learned warm start on the held-out cohort. With ``--train``, the
+    network is first trained on 50 seeded cohorts (N=20,000, M=50,000, K in 6..10, F in
+    0.02..0.15; 5 more choose the epoch) by this library's kernels, targets the converged Q
+    of plain EM from the ALS start, and written to ``--weights-out``; otherwise the shipped
+    weights are used. Then plain EM from the ALS start and EM from the warm start run on the
+    held-out cohort with the default arithmetic: iterations and seconds to the first check
+    within 1e-6 relative of the plain run's converged log-likelihood. One JSON line."""
+    import torch
+
+    from adamixture_b200.model import warm_start as ws
+
+    dev = torch.device("cuda", 0)
+    out = {"metric": "learned warm start vs ALS start", "config": {"workload": cfg["workload"]}}
+    if args.train:
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        rep = ws.train_default(dev, out=args.weights_out, n_train=50, n_val=5, size=(20_000, 50_000), epochs=30)
+        torch.cuda.synchronize()
+        out["training"] = {"seconds": time.perf_counter() - t0, "cohorts": len(rep["cohorts"]),
+                           "train_loss": rep["train_loss"], "val_loss": rep["val_loss"],
+                           "weights": str(args.weights_out)}
+        net = ws.WarmStartMLP.load(args.weights_out, dev)
+    else:
+        net = ws.WarmStartMLP.load(ws.DEFAULT_WEIGHTS, dev)
+    N, M, K = cfg["N"], cfg["M"], cfg["K"]
+    G, _ = ws.simulate(N, M, K, cfg["F"], cfg["seed"], dev, alpha=cfg["alpha"], miss=cfg["miss"])
+    # load the kernel instances the fits use before timing them
+    ws.warm_start_fit(net, G[: (20_000 + 3) // 4], N, 20_000, K, seed=42)
+    r = ws.warm_start_fit(net, G, N, M, K, seed=42)
+    r.pop("P"), r.pop("Q")
+    out["held_out"] = r
+    print(json.dumps(out), flush=True)
+
+
 def run_e2e_dist(args, G_dev, P0, Q0, M_loc, N, K, prec, dev, world):
     """e2e at N GPUs: each rank's packed rows and P rows plus Q from pinned host memory,
     ``optimize_parameters_dist`` for ``steps`` iterations, P rows and Q back to the host;
@@ -1010,6 +1047,9 @@ def main():
                     help="c4: iteration cap of the full-data fits")
     ap.add_argument("--cv-polish", dest="cv_polish", type=int, default=10,
                     help="c4: Adam-EM iterations per fold")
+    ap.add_argument("--train", action="store_true", help="c5: train the warm-start network first")
+    ap.add_argument("--weights-out", dest="weights_out", default="gpurun_out/warm_start_weights.npz",
+                    help="c5 --train: where the trained weights go")
     ap.add_argument("--batch-sweeps", dest="batch_sweeps", action="store_true",
                     help="c4: time single and batched sweep launches instead of the CV runs")
     ap.add_argument("--kernels-skip-hessian", dest="kernels_skip_hessian", action="store_true")
@@ -1041,6 +1081,10 @@ def main():
     if args.config == "c4":
         if rank == 0:
             run_cv_batch(args, cfg)
+        return
+    if args.config == "c5":
+        if rank == 0:
+            run_warm_start(args, cfg)
         return
     if args.sweep_by_k:
         if rank == 0:

@@ -1,6 +1,8 @@
 """The warm-start network on the GPU: forward and gradients of the CUDA kernels against
-the float64 oracle (oracle/mlp.py) with the same BF16 weights (relative 2e-3 of each
-tensor's largest magnitude: float32 accumulation over 256-wide layers and a batch sum),
+the float64 oracle (oracle/mlp.py) with the same BF16 weights and the kernels' BF16
+rounding of every product's inputs (relative 2e-3 of each tensor's largest magnitude: float32
+accumulation over 256-wide layers and a batch sum, and the BF16 rounding of float32 activations
+that differ from the oracle's float64 ones in their last bits),
 the untrained network reproducing its prior, training lowering the loss, the one-step
 M-step against numpy, and a warm-started fit on a held-out cohort (network trained on
 seeded cohorts by these kernels), whose result is never worse than plain EM."""
