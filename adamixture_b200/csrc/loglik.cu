@@ -288,8 +288,10 @@ using namespace adx;
 
 // Float64 with K <= 16: h on the float64 MMA tiles of the float64 sweep (em_sweep_dmma.cu);
 // `nblk` receives its partial count, and partial == nullptr only queries it.
+namespace adx {
 int dmma_loglik(const uint8_t* G, const double* P, const double* Q, int64_t M, int64_t N, int K, double* partial,
                 int* nblk, cudaStream_t st);
+}
 constexpr int LL_DMMA_MAX_K = 16;
 
 extern "C" int adx_loglik_workspace_bytes(int64_t M, int64_t N, int K, int precision, size_t* bytes) {
