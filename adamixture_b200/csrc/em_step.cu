@@ -442,6 +442,7 @@ int em_plan(int64_t M, int64_t N, int K, int prec, EmPlan& pl) {
   int64_t n_split = (int64_t)llround(s);
   n_split = n_split < 1 ? 1 : n_split;
   n_split = n_split > pl.n_stile ? pl.n_stile : n_split;
+  n_split = n_split > PLAN_BLOCKS ? PLAN_BLOCKS : n_split;  // the grid stays within PLAN_BLOCKS
   int64_t max_mblk = ceil_div(M, CH);
   int64_t n_mblk = PLAN_BLOCKS / n_split;  // the grid stays within PLAN_BLOCKS
   n_mblk = n_mblk < 1 ? 1 : (n_mblk > max_mblk ? max_mblk : n_mblk);
