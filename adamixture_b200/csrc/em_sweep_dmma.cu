@@ -10,8 +10,9 @@
 // are float64 MMAs (mma.sync m16n8k4 .f64, 512 FMAs per warp instruction) and the CUDA
 // cores do only the per-entry ratios.
 //
-// CTA: 8 warps over a 256-sample sub-tile, 32 samples per warp, walking the block's SNPs in
-// chunks of 16 (groups of 8 chunks staged in shared memory). Per chunk a warp owns a 16-SNP
+// CTA: 4 warps over a 128-sample sub-tile, 32 samples per warp (two CTAs per SM, so one
+// CTA's chunk barrier does not idle the SM), walking the block's SNPs in chunks of 16
+// (groups of 8 chunks staged in shared memory). Per chunk a warp owns a 16-SNP
 // x 32-sample tile as four 16 x 8 MMA tiles (fragment element: SNP row g or g+8, columns
 // 2t, 2t+1; g = lane / 4, t = lane % 4). Column j of tile nt is local sample
 // 8 (j / 2) + 2 nt + (j % 2), so a thread's 8 entries per SNP row are 8 consecutive
@@ -24,7 +25,7 @@
 //   * d = a - b goes through a per-warp shared-memory transpose (samples x SNPs) to become
 //     the A operand of T += d^T P (16 samples x 8 K-columns, 4 SNPs per k-step); sum_j b
 //     is added per thread and folded over the SNP lanes at the end.
-// A and B of a chunk are summed over the 8 warps in shared memory (fixed order, double
+// A and B of a chunk are summed over the CTA's warps in shared memory (fixed order, double
 // buffered: one barrier per chunk) and added into the block's own AB_part rows; T lives in
 // the MMA accumulators for the whole SNP block and is written once per sub-tile.
 // Shared-memory layouts are chosen so that every fragment load and store is free of bank
@@ -34,7 +35,7 @@
 namespace adx {
 namespace dm {
 
-constexpr int WARPS = 8;
+constexpr int WARPS = 4;
 constexpr int TPB = WARPS * 32;
 constexpr int WS = 32;                 // samples per warp
 constexpr int W = WARPS * WS;          // samples per sub-tile
@@ -45,6 +46,7 @@ constexpr int QSTR = 24;               // Q tile row stride (doubles); column sw
 constexpr int PSTR = 20;               // P tile row stride (doubles)
 constexpr int DSTR = 20;               // transpose tile row stride (doubles); swizzle dsw()
 constexpr int NV = 16;                 // A/B accumulator values per thread (2 x 2 tiles x 4)
+constexpr int RU = NV * 32 / TPB;      // A/B values a thread sums over the warps per chunk
 
 // shared memory (doubles)
 constexpr int Q_OFF = 0;
@@ -190,10 +192,12 @@ __device__ __forceinline__ void sweep_subtile(const Args& a, const Prob& pr, int
         }
         // this thread's two A/B partial sums of the chunk, read now so that the read's
         // latency overlaps the chunk's arithmetic (added after the chunk barrier)
-        double old_ab[2] = {0.0, 0.0};
+        double old_ab[RU];
+#pragma unroll
+        for (int u = 0; u < RU; ++u) old_ab[u] = 0.0;
         if (!first) {
 #pragma unroll
-          for (int u = 0; u < 2; ++u) {
+          for (int u = 0; u < RU; ++u) {
             const int e = threadIdx.x + u * TPB;
             const int v = e >> 5, l = e & 31, n = (v >> 2) & 1, el = v & 3;
             const int row = (l >> 2) + 8 * (el >> 1);
@@ -304,7 +308,7 @@ __device__ __forceinline__ void sweep_subtile(const Args& a, const Prob& pr, int
         // sum over the warps in a fixed order; value v of lane l is (A if v < 8 else B),
         // column tile (v / 4) % 2, element v % 4 of lane l's fragment
 #pragma unroll
-        for (int u = 0; u < 2; ++u) {
+        for (int u = 0; u < RU; ++u) {
           const int e = threadIdx.x + u * TPB;
           const int v = e >> 5, l = e & 31;
           const int n = (v >> 2) & 1;
@@ -372,7 +376,7 @@ __device__ __forceinline__ void sweep_subtile(const Args& a, const Prob& pr, int
 // read it from memory once; a problem's arithmetic and summation order do not depend on the
 // other problems.
 template <int KS, int MAXP>
-__global__ void __launch_bounds__(TPB, 1) em_sweep_dmma_kernel(Args a, Probs<MAXP> ps) {
+__global__ void __launch_bounds__(TPB, 2) em_sweep_dmma_kernel(Args a, Probs<MAXP> ps) {
   extern __shared__ __align__(16) double sm[];
   const int mblk = blockIdx.x % a.n_mblk;
   const int split = blockIdx.x / a.n_mblk;

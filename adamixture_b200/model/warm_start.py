@@ -338,11 +338,12 @@ def warm_start_fit(net: WarmStartMLP, G, N: int, M: int, K: int, seed: int = 42,
 DEFAULT_WEIGHTS = Path(__file__).resolve().parent / "warm_start_weights.npz"
 
 
-def train_default(device, out=DEFAULT_WEIGHTS, n_train: int = 12, n_val: int = 3, size=(6000, 12000),
+def train_default(device, out=DEFAULT_WEIGHTS, n_train: int = 50, n_val: int = 5, size=(20_000, 50_000),
                   epochs: int = 30, seed: int = 0) -> dict:
-    """Train the shipped weights: seeded synthetic cohorts (K in 6..10, F in 0.02..0.15,
-    Dirichlet(0.5) memberships, 1% missing) fitted by plain EM from the ALS start; the
-    last ``n_val`` cohorts select the epoch. Reproducible from the seeds."""
+    """Train the shipped weights: 50 seeded synthetic cohorts of N=20,000 x M=50,000 (K in
+    6..10, F in 0.02..0.15, Dirichlet(0.5) memberships, 1% missing) fitted by plain EM from
+    the ALS start; 5 more cohorts select the epoch. Reproducible from the seeds
+    (``python bench.py --config c5 --train`` runs it and evaluates the result)."""
     rng = np.random.default_rng(seed)
     N, M = size
     spec = [(N, M, int(rng.integers(6, 11)), float(rng.uniform(0.02, 0.15)), 5000 + c)
