@@ -10,9 +10,10 @@
 // are float64 MMAs (mma.sync m16n8k4 .f64, 512 FMAs per warp instruction) and the CUDA
 // cores do only the per-entry ratios.
 //
-// CTA: 4 warps over a 128-sample sub-tile, 32 samples per warp (two CTAs per SM, so one
-// CTA's chunk barrier does not idle the SM), walking the block's SNPs in chunks of 16
-// (groups of 8 chunks staged in shared memory). Per chunk a warp owns a 16-SNP
+// CTA: 8 warps over a 256-sample sub-tile, 32 samples per warp, walking the block's SNPs in
+// chunks of 16 (groups of 8 chunks staged in shared memory). (Two 4-warp CTAs per SM ran
+// at the same speed with 4x the DRAM traffic: twice the A/B partial read-modify-writes,
+// which no longer stayed in L2.) Per chunk a warp owns a 16-SNP
 // x 32-sample tile as four 16 x 8 MMA tiles (fragment element: SNP row g or g+8, columns
 // 2t, 2t+1; g = lane / 4, t = lane % 4). Column j of tile nt is local sample
 // 8 (j / 2) + 2 nt + (j % 2), so a thread's 8 entries per SNP row are 8 consecutive
@@ -35,7 +36,7 @@
 namespace adx {
 namespace dm {
 
-constexpr int WARPS = 4;
+constexpr int WARPS = 8;
 constexpr int TPB = WARPS * 32;
 constexpr int WS = 32;                 // samples per warp
 constexpr int W = WARPS * WS;          // samples per sub-tile
@@ -376,7 +377,7 @@ __device__ __forceinline__ void sweep_subtile(const Args& a, const Prob& pr, int
 // read it from memory once; a problem's arithmetic and summation order do not depend on the
 // other problems.
 template <int KS, int MAXP>
-__global__ void __launch_bounds__(TPB, 2) em_sweep_dmma_kernel(Args a, Probs<MAXP> ps) {
+__global__ void __launch_bounds__(TPB, 1) em_sweep_dmma_kernel(Args a, Probs<MAXP> ps) {
   extern __shared__ __align__(16) double sm[];
   const int mblk = blockIdx.x % a.n_mblk;
   const int split = blockIdx.x / a.n_mblk;
