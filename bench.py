@@ -61,7 +61,7 @@ CONFIGS = {
     "c4": dict(workload="K sweep K=2..12 with 5-fold CV (10 % of entries per fold, seeded hash), N=20000 samples, M=100000 SNPs, true K=6, F=0.08, Q Dir(0.5), 1% missing",
                N=20_000, M=100_000, K=6, F=0.08, alpha=0.5, miss=0.01, seed=4000),
     "c5": dict(workload="learned warm start vs the ALS start, held-out cohort N=100000 samples, M=300000 SNPs, K=8, F=0.05, Q Dir(0.5), 1% missing",
-               N=100_000, M=300_000, K=8, F=0.05, alpha=0.5, miss=0.01, seed=5000),
+               N=100_000, M=300_000, K=8, F=0.05, alpha=0.5, miss=0.01, seed=6000),
     # the c3 cohort's generator at one tenth of its SNPs (2.5 GB packed): the size profiled
     # under ncu, whose full capture saves and restores device memory on every pass
     "c3s": dict(workload="Adam-EM, N=200000 samples, M=50000 SNPs, K=10, F=0.02, Q 0.7*Dir(0.05)+0.3*Dir(1), 1% missing",
