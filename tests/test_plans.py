@@ -7,6 +7,9 @@ only; no GPU needed).
   here as a greedy list schedule and compared with the library's choice.
 * Log-likelihood: the grid never exceeds 1776 blocks (148 x 12), so its partial sums
   always fit the allocation-free variant's 2048-entry array.
+* Batched float64 E-step: its workspace is every problem's single-problem partials side by
+  side (the float64 plan does not depend on K), and it rejects K > 16 and more than 64
+  problems.
 """
 import heapq
 
@@ -92,3 +95,42 @@ def test_loglik_grid_stays_within_the_partials_bound(prec):
                 assert 1 <= blocks <= LL_BLOCKS, (M, N, K, blocks)
                 worst = max(worst, blocks)
     assert worst <= NOALLOC_PARTIALS
+
+
+def _batch_bytes(M, N, Ks):
+    import ctypes
+
+    arr = (ctypes.c_int * len(Ks))(*Ks)
+    return _lib.query_size("adx_em_batch_workspace_bytes", M, N, len(Ks), ctypes.addressof(arr))
+
+
+@pytest.mark.parametrize("M,N", [(100_000, 20_000), (3_001, 4_096), (33, 1_000_000), (500_000, 200_000)])
+def test_batch_workspace_is_the_single_problem_partials_side_by_side(M, N):
+    # the float64 plan does not depend on K, so a batch's workspace is a 256-byte header plus
+    # every problem's single-problem partials (each 256-byte aligned)
+    Ks = [2, 7, 10, 12, 16, 1]
+    header = 256
+    total = header
+    for K in Ks:
+        single = _lib.query_size("adx_em_workspace_bytes", M, N, K, _lib.ADX_F64)
+        total += cdiv(single - header, 256) * 256
+    assert _batch_bytes(M, N, Ks) == total
+
+
+def test_batch_rejects_what_it_cannot_run():
+    with pytest.raises(_lib.AdxError, match="invalid argument"):
+        _batch_bytes(1000, 1000, [17])          # the batched sweep is the K <= 16 float64 form
+    with pytest.raises(_lib.AdxError, match="invalid argument"):
+        _batch_bytes(1000, 1000, [4] * 65)      # at most 64 problems per launch
+    with pytest.raises(_lib.AdxError, match="invalid argument"):
+        _batch_bytes(1000, 1000, [0])
+
+
+def test_float64_plan_stays_within_the_block_bound():
+    # the E-step plan's grid (sample splits x SNP blocks) never exceeds 1776 blocks, including
+    # a single SNP row against a million samples
+    for M in (1, 16, 1_000, 500_000):
+        for N in (1, 257, 200_000, 1_000_000):
+            for K in (3, 10, 16, 40):
+                nbytes = _lib.query_size("adx_loglik_workspace_bytes", M, N, K, _lib.ADX_F64)
+                assert (nbytes - 256) // 8 <= LL_BLOCKS, (M, N, K)
