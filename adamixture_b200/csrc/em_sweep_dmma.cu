@@ -214,22 +214,11 @@ __device__ __forceinline__ void sweep_subtile(const Args& a, const Prob& pr, int
           ph[ks][0] = ks < ksp ? pc[g * PSTR + 4 * ks + t] : 0.0;
           ph[ks][1] = ks < ksp ? pc[(g + 8) * PSTR + 4 * ks + t] : 0.0;
         }
-        // A/B columns 8.. on the MMA only when K > 12; for 8 < K <= 12 the NX = K - 8 columns
-        // past the first tile are summed on the CUDA cores (ax, bx: rows g and g+8 of this
-        // thread's samples), which saves 16 of the chunk's 60 MMAs at K = 9..12
-        constexpr bool XCOL = KS == 3;
-        constexpr int NKM = XCOL ? 1 : NK;
-        const int nx = XCOL ? K - 8 : 0;
-        double aacc[NKM][4], bacc[NKM][4];
+        double aacc[NK][4], bacc[NK][4];
 #pragma unroll
-        for (int n = 0; n < NKM; ++n)
+        for (int n = 0; n < NK; ++n)
 #pragma unroll
           for (int e = 0; e < 4; ++e) aacc[n][e] = bacc[n][e] = 0.0;
-        double ax[2][4], bx[2][4];
-#pragma unroll
-        for (int h = 0; h < 2; ++h)
-#pragma unroll
-          for (int c = 0; c < 4; ++c) ax[h][c] = bx[h][c] = 0.0;
 
         // H of tile nt + 1 is issued before tile nt's ratios, so the MMAs' latency overlaps them
         double hcur[4] = {0.0, 0.0, 0.0, 0.0}, hnext[4];
@@ -278,23 +267,11 @@ __device__ __forceinline__ void sweep_subtile(const Args& a, const Prob& pr, int
           for (int c = 0; c < 2; ++c) {
             const int qrow = warp * WS + 8 * t + 2 * nt + c;
 #pragma unroll
-            for (int n = 0; n < NKM; ++n) {
+            for (int n = 0; n < NK; ++n) {
               if (n >= nkp) continue;
               const double qb = qt[qrow * QSTR + ((8 * n + g) ^ qsw(qrow))];
               mma_f64(aacc[n], av[c], av[2 + c], qb);
               mma_f64(bacc[n], bv[c], bv[2 + c], qb);
-            }
-            if constexpr (XCOL) {
-              // columns 8 + x of this thread's sample 8t + 2nt + c, rows g (e = c) and g+8 (e = 2 + c)
-#pragma unroll
-              for (int x = 0; x < 4; ++x) {
-                if (x >= nx) continue;
-                const double qx = qt[qrow * QSTR + ((8 + x) ^ qsw(qrow))];
-                ax[0][x] = fma(av[c], qx, ax[0][x]);
-                ax[1][x] = fma(av[2 + c], qx, ax[1][x]);
-                bx[0][x] = fma(bv[c], qx, bx[0][x]);
-                bx[1][x] = fma(bv[2 + c], qx, bx[1][x]);
-              }
             }
           }
           if (nt < 3) {
@@ -322,35 +299,12 @@ __device__ __forceinline__ void sweep_subtile(const Args& a, const Prob& pr, int
         // A/B of the chunk: this warp's share into the reduction buffer
         double* red = sm + R_OFF + (chunk_no & 1) * (WARPS * NV * 32);
 #pragma unroll
-        for (int n = 0; n < NKM; ++n)
+        for (int n = 0; n < NK; ++n)
 #pragma unroll
           for (int e = 0; e < 4; ++e) {
             red[(warp * NV + n * 4 + e) * 32 + lane] = aacc[n][e];
             red[(warp * NV + 8 + n * 4 + e) * 32 + lane] = bacc[n][e];
           }
-        if constexpr (XCOL) {
-          // the CUDA-core columns summed over the four lanes of each row group (t), then
-          // stored where the second column tile's fragment would hold them: lane (g, t),
-          // element e is row g + 8(e/2), column 8 + 2t + e%2
-#pragma unroll
-          for (int h = 0; h < 2; ++h)
-#pragma unroll
-            for (int x = 0; x < 4; ++x) {
-              ax[h][x] += __shfl_xor_sync(0xffffffffu, ax[h][x], 1);
-              ax[h][x] += __shfl_xor_sync(0xffffffffu, ax[h][x], 2);
-              bx[h][x] += __shfl_xor_sync(0xffffffffu, bx[h][x], 1);
-              bx[h][x] += __shfl_xor_sync(0xffffffffu, bx[h][x], 2);
-            }
-#pragma unroll
-          for (int e = 0; e < 4; ++e) {
-            const int h = e >> 1, lo = e & 1;
-            // column 8 + 2t + lo: x = 2t + lo, picked without indexing registers by t
-            const double av2 = t == 0 ? ax[h][lo] : ax[h][2 + lo];
-            const double bv2 = t == 0 ? bx[h][lo] : bx[h][2 + lo];
-            red[(warp * NV + 4 + e) * 32 + lane] = t < 2 ? av2 : 0.0;
-            red[(warp * NV + 12 + e) * 32 + lane] = t < 2 ? bv2 : 0.0;
-          }
-        }
         __syncthreads();
         // sum over the warps in a fixed order; value v of lane l is (A if v < 8 else B),
         // column tile (v / 4) % 2, element v % 4 of lane l's fragment
