@@ -400,7 +400,7 @@ int dmma_plan_width();
 int dmma_plan_chunk();
 int dmma_sweep(const uint8_t* G, const double* P, const double* Q, int64_t M, int64_t N, int K,
                int64_t n_stile, int n_split, int n_mblk, int64_t mb, double* ABp, double* Tp,
-               cudaStream_t st);
+               cudaStream_t st, double* llp = nullptr);
 // Float64 sweeps for K <= 16 run on the float64 tensor-core MMA (em_sweep_dmma.cu).
 constexpr int DMMA_MAX_K = 16;
 
@@ -453,6 +453,8 @@ int em_plan(int64_t M, int64_t N, int K, int prec, EmPlan& pl) {
   pl.mb = mb;
   pl.ab_elems = (size_t)n_split * (size_t)M * 2 * K;
   pl.t_elems = (size_t)n_mblk * (size_t)N * K;
+  // the float64 tensor-core sweep can also leave one log-likelihood partial per CTA
+  if (prec == ADX_F64 && K <= DMMA_MAX_K) pl.extra_bytes = (size_t)n_split * (size_t)n_mblk * sizeof(double);
   return ADX_OK;
 }
 
@@ -682,6 +684,88 @@ extern "C" int adx_em_adam_iteration(const uint8_t* G, int64_t M, int64_t N, int
   if (rc) return rc;
   return em_update(pl, workspace, 1, nullptr, nullptr, nullptr, q_bat, P, Q, P32, Q32, mP, vP, mQ,
                    vQ, AdamArgs{t, lr, beta1, beta2, eps}, st);
+}
+
+// ---------------------------------------------------------------- sweep + log-likelihood
+//
+// The reference checks the log-likelihood of (P, Q) after an iteration's Adam move, and the
+// next iteration's E-step sweeps the same (P, Q). adx_em_sweep_loglik is that sweep with the
+// check folded in (float64, K <= 16): the same partials as adx_em_sweep plus the log-
+// likelihood of its input, bit-identical to adx_loglik's float64 form; the optimiser reads
+// it (adx_em_loglik_from_sweep), takes its decisions, then applies the move
+// (adx_em_adam_update), so a check costs no pass of its own.
+
+namespace adx {
+// The partials' sum in the order adx_loglik's final sum uses (256 strided sums, then a tree),
+// so the two log-likelihoods are bit-identical.
+__global__ void ll_sum_kernel(const double* __restrict__ partial, int n, double* __restrict__ out) {
+  __shared__ double sh[256];
+  double s = 0.0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) s += partial[i];
+  sh[threadIdx.x] = s;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w >= 1; w >>= 1) {
+    if ((int)threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) *out = sh[0];
+}
+}  // namespace adx
+
+static int ll_layout(const EmPlan& pl, void* ws, double** llp) {
+  if (pl.prec != ADX_F64 || pl.K > DMMA_MAX_K) return ADX_ERR_UNSUPPORTED;
+  *llp = reinterpret_cast<double*>(static_cast<uint8_t*>(ws) + pl.extra_offset());
+  return ADX_OK;
+}
+
+extern "C" int adx_em_sweep_loglik(const uint8_t* G, int64_t M, int64_t N, int K, int precision, const void* P,
+                                   const void* Q, void* workspace, size_t workspace_bytes, void* stream) {
+  EmPlan pl;
+  int rc = em_plan(M, N, K, precision, pl);
+  if (rc) { adx_set_message("adx_em_sweep_loglik: bad shape or precision"); return rc; }
+  if (!G || !P || !Q || !workspace) { adx_set_message("adx_em_sweep_loglik: null pointer"); return ADX_ERR_ARG; }
+  if (workspace_bytes < pl.bytes()) { adx_set_message("adx_em_sweep_loglik: workspace too small"); return ADX_ERR_WORKSPACE; }
+  double* llp = nullptr;
+  if (ll_layout(pl, workspace, &llp)) {
+    adx_set_message("adx_em_sweep_loglik: float64 with K <= 16 only");
+    return ADX_ERR_UNSUPPORTED;
+  }
+  double* ABp = reinterpret_cast<double*>(static_cast<uint8_t*>(workspace) + EmPlan::HEADER);
+  return dmma_sweep(G, (const double*)P, (const double*)Q, M, N, K, pl.n_stile, pl.n_split, pl.n_mblk, pl.mb, ABp,
+                    ABp + pl.ab_elems, as_stream(stream), llp);
+}
+
+extern "C" int adx_em_loglik_from_sweep(void* workspace, size_t workspace_bytes, int64_t M, int64_t N, int K,
+                                        int precision, double* out, void* stream) {
+  EmPlan pl;
+  int rc = em_plan(M, N, K, precision, pl);
+  if (rc) { adx_set_message("adx_em_loglik_from_sweep: bad shape or precision"); return rc; }
+  if (!workspace || !out) { adx_set_message("adx_em_loglik_from_sweep: null pointer"); return ADX_ERR_ARG; }
+  if (workspace_bytes < pl.bytes()) { adx_set_message("adx_em_loglik_from_sweep: workspace too small"); return ADX_ERR_WORKSPACE; }
+  double* llp = nullptr;
+  if (ll_layout(pl, workspace, &llp)) {
+    adx_set_message("adx_em_loglik_from_sweep: float64 with K <= 16 only");
+    return ADX_ERR_UNSUPPORTED;
+  }
+  ll_sum_kernel<<<1, 256, 0, as_stream(stream)>>>(llp, pl.n_split * pl.n_mblk, out);
+  ADX_LAUNCH_CHECK();
+  return ADX_OK;
+}
+
+extern "C" int adx_em_adam_update(int64_t M, int64_t N, int K, int precision, double* P, double* Q, float* P32,
+                                  float* Q32, double* mP, double* vP, double* mQ, double* vQ, const double* q_bat,
+                                  double t, double lr, double beta1, double beta2, double eps, void* workspace,
+                                  size_t workspace_bytes, void* stream) {
+  EmPlan pl;
+  int rc = em_plan(M, N, K, precision, pl);
+  if (rc) { adx_set_message("adx_em_adam_update: bad shape or precision"); return rc; }
+  if (!P || !Q || !mP || !vP || !mQ || !vQ || !q_bat || !workspace || t < 1) {
+    adx_set_message("adx_em_adam_update: bad arguments");
+    return ADX_ERR_ARG;
+  }
+  if (workspace_bytes < pl.bytes()) { adx_set_message("adx_em_adam_update: workspace too small"); return ADX_ERR_WORKSPACE; }
+  return em_update(pl, workspace, 1, nullptr, nullptr, nullptr, q_bat, P, Q, P32, Q32, mP, vP, mQ, vQ,
+                   AdamArgs{t, lr, beta1, beta2, eps}, as_stream(stream));
 }
 
 // The float64 log-likelihood on the float64 MMA (em_sweep_dmma.cu) uses the float64 sweep's

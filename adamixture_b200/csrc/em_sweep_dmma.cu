@@ -106,7 +106,52 @@ struct Args {
   int64_t n_stile;
   int n_split, n_mblk;
   int64_t mb;
+  double* llp;        // the sweep with the log-likelihood: one partial per CTA
 };
+
+// Split x = m * 2^e with m in [0.5, 1): returns m, adds e to e.
+__device__ __forceinline__ double renorm_dm(double x, int& e) {
+  int hi = __double2hiint(x);
+  const int lo = __double2loint(x);
+  e += ((hi >> 20) & 0x7FF) - 1022;
+  hi = (hi & 0x800FFFFF) | (1022 << 20);
+  return __hiloint2double(hi, lo);
+}
+
+// The log-likelihood factor h^g (1-h)^(2-g) of 4 entries (1 when missing), h clamped to
+// [1e-10, 1-1e-10], multiplied into the thread's running product.
+__device__ __forceinline__ void ll_factors(const double (&hacc)[4], const uint64_t (&w)[2], int nt, double& prod,
+                                           int& ex) {
+  double f[4];
+#pragma unroll
+  for (int e = 0; e < 4; ++e) {
+    const uint32_t code = (uint32_t)(w[e >> 1] >> (8 * (2 * nt + (e & 1)))) & 3u;
+    const double h = fmin(fmax(hacc[e], LL_CLAMP), 1.0 - LL_CLAMP);
+    const double om = 1.0 - h;
+    const double x = code == 2u ? h : om;
+    const double y = code == 0u ? om : h;
+    f[e] = code == 3u ? 1.0 : x * y;
+  }
+  prod *= (f[0] * f[1]) * (f[2] * f[3]);
+  prod = renorm_dm(prod, ex);
+}
+
+// The CTA's log-likelihood partial: each thread's log(prod) + ex ln 2, summed over the warp
+// by shuffles and over the warps in order.
+__device__ __forceinline__ void ll_block_sum(double prod, int ex, double* wsum, double* out) {
+  double acc = log(prod) + (double)ex * 0.69314718055994530942;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  __syncthreads();
+  if (lane == 0) wsum[warp] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s = 0.0;
+    for (int w2 = 0; w2 < WARPS; ++w2) s += wsum[w2];
+    *out = s;
+  }
+}
 
 // One E-step problem: its packed genotypes (cross-validation folds pass a copy with the
 // fold's entries hidden), P [M][K] and Q [N][K] (float64), and its partial sums.
@@ -129,9 +174,11 @@ struct Probs {
 // KS: k-steps of 4 covering the problem's K (K <= 4 KS); NK = ceil(KS / 2) column tiles of
 // 8. One (problem, sample sub-tile) of a CTA: the sub-tile's Q rows, then the CTA's SNP
 // block in groups of 8 chunks of 16 SNPs, then the sub-tile's T partials.
-template <int KS>
+// LL: also multiply every entry's log-likelihood factor into (prod, ex), in the order and
+// arithmetic of loglik_dmma_kernel, so the CTA's partial equals that kernel's.
+template <int KS, bool LL>
 __device__ __forceinline__ void sweep_subtile(const Args& a, const Prob& pr, int64_t st, int split, int mblk,
-                                              int& chunk_no, double* sm) {
+                                              int& chunk_no, double* sm, double& prod, int& ex) {
   constexpr int NK = (KS + 1) / 2;
   double* qt = sm + Q_OFF;   // [W][QSTR]: Q rows of the sub-tile, columns swizzled by qsw(row)
   double* pt = sm + P_OFF;   // [GS][PSTR]: P rows of the group
@@ -239,6 +286,7 @@ __device__ __forceinline__ void sweep_subtile(const Args& a, const Prob& pr, int
               if (ks < ksp) mma_f64(hnext, ph[ks][0], ph[ks][1], qt[qrow_h * QSTR + ((4 * ks + t) ^ qsw(qrow_h))]);
           }
           const double (&hacc)[4] = hcur;
+          if constexpr (LL) ll_factors(hacc, w, nt, prod, ex);
           double av[4], bv[4];
 #pragma unroll
           for (int e = 0; e < 4; ++e) {
@@ -376,27 +424,33 @@ __device__ __forceinline__ void sweep_subtile(const Args& a, const Prob& pr, int
 // genotypes find the CTA's genotype region (about 0.3 MB at N=20k, M=100k) still in L2 and
 // read it from memory once; a problem's arithmetic and summation order do not depend on the
 // other problems.
-template <int KS, int MAXP>
+// LL (single problem only): the sweep also sums the log-likelihood of its input (P, Q) into
+// a.llp[blockIdx.x], bit-identical to loglik_dmma_kernel's partials.
+template <int KS, int MAXP, bool LL>
 __global__ void __launch_bounds__(TPB, 1) em_sweep_dmma_kernel(Args a, Probs<MAXP> ps) {
+  static_assert(!LL || MAXP == 1, "the log-likelihood rides on single-problem sweeps");
   extern __shared__ __align__(16) double sm[];
   const int mblk = blockIdx.x % a.n_mblk;
   const int split = blockIdx.x / a.n_mblk;
   int chunk_no = 0;   // parity of the A/B reduction buffer
+  double prod = 1.0;
+  int ex = 0;
   for (int pi = 0; pi < (MAXP == 1 ? 1 : ps.n); ++pi) {
     const Prob pr = ps.p[pi];
     for (int64_t st = split; st < a.n_stile; st += a.n_split) {
       if constexpr (MAXP == 1) {
-        sweep_subtile<KS>(a, pr, st, split, mblk, chunk_no, sm);
+        sweep_subtile<KS, LL>(a, pr, st, split, mblk, chunk_no, sm, prod, ex);
       } else {
         switch ((pr.K + 3) >> 2) {
-          case 1: sweep_subtile<1>(a, pr, st, split, mblk, chunk_no, sm); break;
-          case 2: sweep_subtile<2>(a, pr, st, split, mblk, chunk_no, sm); break;
-          case 3: sweep_subtile<3>(a, pr, st, split, mblk, chunk_no, sm); break;
-          default: sweep_subtile<4>(a, pr, st, split, mblk, chunk_no, sm); break;
+          case 1: sweep_subtile<1, false>(a, pr, st, split, mblk, chunk_no, sm, prod, ex); break;
+          case 2: sweep_subtile<2, false>(a, pr, st, split, mblk, chunk_no, sm, prod, ex); break;
+          case 3: sweep_subtile<3, false>(a, pr, st, split, mblk, chunk_no, sm, prod, ex); break;
+          default: sweep_subtile<4, false>(a, pr, st, split, mblk, chunk_no, sm, prod, ex); break;
         }
       }
     }
   }
+  if constexpr (LL) ll_block_sum(prod, ex, sm + S_OFF, a.llp + blockIdx.x);
 }
 
 // ---------------------------------------------------------------- float64 log-likelihood
@@ -408,14 +462,6 @@ __global__ void __launch_bounds__(TPB, 1) em_sweep_dmma_kernel(Args a, Probs<MAX
 // two bits; 1 when missing) into one float64 running product, moves its exponent into an
 // integer after every 4 factors (>= 1e-80 together, so the product stays normal), and takes
 // one log at the end; per-CTA sums in a fixed order, per-CTA partials summed in block order.
-
-__device__ __forceinline__ double renorm_dm(double x, int& e) {
-  int hi = __double2hiint(x);
-  const int lo = __double2loint(x);
-  e += ((hi >> 20) & 0x7FF) - 1022;
-  hi = (hi & 0x800FFFFF) | (1022 << 20);
-  return __hiloint2double(hi, lo);
-}
 
 // shared memory of the log-likelihood: the Q and P tiles and the warp sums (doubles)
 constexpr int LL_SMEM_DOUBLES = P_OFF + GS * PSTR + WARPS;
@@ -487,35 +533,11 @@ __global__ void __launch_bounds__(TPB, 2) loglik_dmma_kernel(Args a, const uint8
             mma_f64(hacc[nt], ph[ks][0], ph[ks][1], qt[qrow * QSTR + ((4 * ks + t) ^ qsw(qrow))]);
         }
 #pragma unroll
-        for (int nt = 0; nt < 4; ++nt) {
-          double f[4];
-#pragma unroll
-          for (int e = 0; e < 4; ++e) {
-            const uint32_t code = (uint32_t)(w[e >> 1] >> (8 * (2 * nt + (e & 1)))) & 3u;
-            const double h = fmin(fmax(hacc[nt][e], LL_CLAMP), 1.0 - LL_CLAMP);
-            const double om = 1.0 - h;
-            const double x = code == 2u ? h : om;
-            const double y = code == 0u ? om : h;
-            f[e] = code == 3u ? 1.0 : x * y;
-          }
-          prod *= (f[0] * f[1]) * (f[2] * f[3]);
-          prod = renorm_dm(prod, ex);
-        }
+        for (int nt = 0; nt < 4; ++nt) ll_factors(hacc[nt], w, nt, prod, ex);
       }
     }
   }
-  double acc = log(prod) + (double)ex * 0.69314718055994530942;
-  // fixed-order block sum: warps by shuffles, then the 8 warp sums in order
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-  __syncthreads();
-  if (lane == 0) wsum[warp] = acc;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    double s = 0.0;
-    for (int w2 = 0; w2 < WARPS; ++w2) s += wsum[w2];
-    partial[blockIdx.x] = s;
-  }
+  ll_block_sum(prod, ex, wsum, partial + blockIdx.x);
 }
 
 }  // namespace dm
@@ -523,17 +545,17 @@ __global__ void __launch_bounds__(TPB, 2) loglik_dmma_kernel(Args a, const uint8
 int dmma_plan_width() { return dm::W; }
 int dmma_plan_chunk() { return dm::CH; }
 
-template <int KS, int MAXP>
+template <int KS, int MAXP, bool LL = false>
 static int dmma_launch(const dm::Args& a, const dm::Probs<MAXP>& ps, cudaStream_t st) {
   static bool attr_set[64] = {false};
   int dev = 0;
   ADX_CUDA_TRY(cudaGetDevice(&dev));
   if (dev >= 0 && dev < 64 && !attr_set[dev]) {
-    ADX_CUDA_TRY(cudaFuncSetAttribute(dm::em_sweep_dmma_kernel<KS, MAXP>,
+    ADX_CUDA_TRY(cudaFuncSetAttribute(dm::em_sweep_dmma_kernel<KS, MAXP, LL>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dm::SMEM_BYTES));
     attr_set[dev] = true;
   }
-  dm::em_sweep_dmma_kernel<KS, MAXP><<<(unsigned)(a.n_split * a.n_mblk), dm::TPB, dm::SMEM_BYTES, st>>>(a, ps);
+  dm::em_sweep_dmma_kernel<KS, MAXP, LL><<<(unsigned)(a.n_split * a.n_mblk), dm::TPB, dm::SMEM_BYTES, st>>>(a, ps);
   ADX_LAUNCH_CHECK();
   return ADX_OK;
 }
@@ -542,20 +564,23 @@ static int dmma_vec(const uint8_t* G, int64_t N) {
   return ((N & 7) == 0 && (reinterpret_cast<uintptr_t>(G) & 7) == 0) ? 1 : 0;
 }
 
+// llp != nullptr: the sweep also writes one log-likelihood partial of its input per CTA.
 int dmma_sweep(const uint8_t* G, const double* P, const double* Q, int64_t M, int64_t N, int K,
                int64_t n_stile, int n_split, int n_mblk, int64_t mb, double* ABp, double* Tp,
-               cudaStream_t st) {
+               cudaStream_t st, double* llp) {
   if (K < 1 || K > 16) return ADX_ERR_UNSUPPORTED;
-  const dm::Args a{M, N, n_stile, n_split, n_mblk, mb};
+  const dm::Args a{M, N, n_stile, n_split, n_mblk, mb, llp};
   dm::Probs<1> ps;
   ps.p[0] = dm::Prob{G, P, Q, ABp, Tp, K, dmma_vec(G, N)};
   ps.n = 1;
+#define ADX_DM_ONE(KS) return llp ? dmma_launch<KS, 1, true>(a, ps, st) : dmma_launch<KS, 1, false>(a, ps, st)
   switch ((K + 3) / 4) {
-    case 1: return dmma_launch<1, 1>(a, ps, st);
-    case 2: return dmma_launch<2, 1>(a, ps, st);
-    case 3: return dmma_launch<3, 1>(a, ps, st);
-    default: return dmma_launch<4, 1>(a, ps, st);
+    case 1: ADX_DM_ONE(1);
+    case 2: ADX_DM_ONE(2);
+    case 3: ADX_DM_ONE(3);
+    default: ADX_DM_ONE(4);
   }
+#undef ADX_DM_ONE
 }
 
 constexpr int DMMA_MAX_PROBLEMS = 64;
@@ -564,7 +589,7 @@ int dmma_sweep_batch(int64_t M, int64_t N, int n, const int* K, const uint8_t* c
                      const double* const* Q, double* const* ABp, double* const* Tp, int64_t n_stile, int n_split,
                      int n_mblk, int64_t mb, cudaStream_t st) {
   if (n < 1 || n > DMMA_MAX_PROBLEMS) return ADX_ERR_ARG;
-  const dm::Args a{M, N, n_stile, n_split, n_mblk, mb};
+  const dm::Args a{M, N, n_stile, n_split, n_mblk, mb, nullptr};
   dm::Probs<DMMA_MAX_PROBLEMS> ps;
   for (int p = 0; p < n; ++p) {
     if (K[p] < 1 || K[p] > 16 || !G[p]) return ADX_ERR_ARG;
@@ -591,7 +616,7 @@ int dmma_loglik(const uint8_t* G, const double* P, const double* Q, int64_t M, i
   if (rc) return rc;
   *nblk = n_split * n_mblk;
   if (!partial) return ADX_OK;
-  const dm::Args a{M, N, n_stile, n_split, n_mblk, mb};
+  const dm::Args a{M, N, n_stile, n_split, n_mblk, mb, nullptr};
   const int vec = dmma_vec(G, N);
 #define ADX_LL_DM(KS)                                                                                          \
   {                                                                                                            \

@@ -137,6 +137,25 @@ class EMAdamOptimizer:
         ops.adam_step(P, Q, P_target, Q_target, self.m_P, self.v_P, self.m_Q, self.v_Q,
                       self._t, self.lr, self.beta1, self.beta2, self.reg_adam, P32, Q32)
 
+    def can_fold_check(self, K: int) -> bool:
+        """Whether this arithmetic has the sweep with the log-likelihood check folded in."""
+        return self.precision == "f64" and K <= 16
+
+    def sweep_with_loglik(self, G, P, Q, M, workspace):
+        """The E-step sweep of the next iteration, which also returns (as a device scalar) the
+        float64 log-likelihood of its input (P, Q): the check the reference runs after the
+        previous iteration's move, bit-identical to ``loglikelihood_gpu``. Follow it with
+        ``apply_update``."""
+        self._sample_counts(G, M)
+        ops.em_sweep_loglik(G, P, Q, M, workspace)
+        return ops.em_loglik_from_sweep(workspace, M, Q.shape[0], Q.shape[1])
+
+    def apply_update(self, P, Q, P32, Q32, M, workspace):
+        """EM targets + Adam move from the last ``sweep_with_loglik`` (at ``self.lr``)."""
+        self._t += 1
+        ops.em_adam_update(P, Q, P32, Q32, self.m_P, self.v_P, self.m_Q, self.v_Q, self.q_bat, M, self._t,
+                           self.lr, self.beta1, self.beta2, self.reg_adam, self.precision, workspace)
+
     def fused_iteration(self, G, P, Q, P32, Q32, M, workspace=None):
         """``run_em_step`` + ``step`` in two launches, without materialising A/B/T."""
         self._sample_counts(G, M)
@@ -167,7 +186,7 @@ def loglikelihood_gpu(G, P, Q, M, N, batch_size, device, threads_per_block, prec
 
 def _optimize_parameters_gpu_once(G, P, Q, lr, beta1, beta2, reg_adam, max_iter, check, K, M, N,
                                   lr_decay, min_lr, patience, tol_adam, device, chunk_size,
-                                  threads_per_block, precision=None, trace=None):
+                                  threads_per_block, precision=None, trace=None, fold_checks=True):
     """Adam-EM with lr decay (em_adam_gpu.py:281-356), fused iterations.
 
     Same control flow as the reference: priming (E-step + Adam step), log-likelihood of
@@ -202,6 +221,9 @@ def _optimize_parameters_gpu_once(G, P, Q, lr, beta1, beta2, reg_adam, max_iter,
     t_start = time.perf_counter()
     opt.fused_iteration(G, P, Q, P32, Q32, M, ws)
     log.info(f"    Performed priming iteration... ({time.time() - ts:.1f}s)\n")
+    if fold_checks and not mixed and opt.can_fold_check(K):
+        return _loop_folded_checks(G, P, Q, M, N, K, opt, ws, max_iter, check, lr_decay, min_lr, patience,
+                                   tol_adam, trace, t_start)
     L_best = loglik()
     P_best, Q_best = P.clone(), Q.clone()
     wait_lr = 0
@@ -240,6 +262,69 @@ def _optimize_parameters_gpu_once(G, P, Q, lr, beta1, beta2, reg_adam, max_iter,
                     wait_lr = 0
     log.info(f"\n    Final log-likelihood: {L_best:.1f}")
     return P_best, Q_best
+
+
+def _loop_folded_checks(G, P, Q, M, N, K, opt, ws, max_iter, check, lr_decay, min_lr, patience, tol_adam, trace,
+                        t_start):
+    """The reference loop after the priming step (em_adam_gpu.py:318-353) with every
+    log-likelihood check folded into the next iteration's sweep (float64, K <= 16).
+
+    The check after iteration ``it`` (1-based ``it`` a multiple of ``check``) scores the
+    (P, Q) that iteration ``it + 1`` sweeps, so that sweep returns it; the decisions (best
+    checkpoint of the current P, Q, learning-rate decay, stop) are taken before that
+    iteration's move is applied, and a stop leaves the move unapplied -- the same states,
+    values and control flow as checking after the move. The first best is the log-likelihood
+    of the primed (P, Q), which the first iteration's sweep returns. A check due after the
+    last iteration runs on its own."""
+    state = {"L_best": None, "P_best": None, "Q_best": None, "wait": 0}
+
+    def decide(L, it):
+        """The reference's decisions on check value L of iteration ``it``; False = stop."""
+        st = ops.em_status(ws, M, N, K, opt.precision)
+        if st:
+            raise RuntimeError(f"E-step sweep reported status {st} (a bounded wait timed out)")
+        if state["L_best"] is None:
+            state["L_best"], state["P_best"], state["Q_best"] = L, P.clone(), Q.clone()
+            return True
+        if trace is not None:
+            trace.append((it, L, time.perf_counter() - t_start))
+        log.info(f"    Iteration {it}, Log-likelihood: {L:.1f}")
+        if L > state["L_best"] + tol_adam:
+            state["L_best"] = L
+            state["P_best"].copy_(P)
+            state["Q_best"].copy_(Q)
+            state["wait"] = 0
+            return True
+        state["wait"] += 1
+        if state["wait"] >= patience:
+            old = opt.lr
+            opt.lr = max(opt.lr * lr_decay, min_lr)
+            log.info(f"    Plateau reached ({state['wait']} checks without beating best). "
+                     f"Reducing lr: {old:.3e} → {opt.lr:.3e}")
+            if opt.lr <= min_lr:
+                log.info("        Convergence reached.")
+                return False
+            state["wait"] = 0
+        return True
+
+    need = True   # the next sweep's input needs its log-likelihood (first: the primed point)
+    stopped = False
+    for it in range(max_iter):
+        if need:
+            L = float(opt.sweep_with_loglik(G, P, Q, M, ws).item())
+            if not decide(L, it):
+                stopped = True
+                break
+            opt.apply_update(P, Q, None, None, M, ws)
+            need = False
+        else:
+            opt.fused_iteration(G, P, Q, None, None, M, ws)
+        if (it + 1) % check == 0:
+            need = True
+    if need and not stopped:
+        decide(float(ops.loglik_device(G, P, Q, M, "f64").item()), max_iter)
+    log.info(f"\n    Final log-likelihood: {state['L_best']:.1f}")
+    return state["P_best"], state["Q_best"]
 
 
 def optimize_parameters_gpu(G, P, Q, lr, beta1, beta2, reg_adam, max_iter, check, K, M, N,

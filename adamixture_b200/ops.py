@@ -203,6 +203,31 @@ def em_sweep(G: torch.Tensor, P: torch.Tensor, Q: torch.Tensor, M: int, precisio
          workspace.data_ptr(), workspace.numel(), _stream(G.device))
 
 
+def em_sweep_loglik(G: torch.Tensor, P: torch.Tensor, Q: torch.Tensor, M: int, workspace: torch.Tensor) -> None:
+    """The float64 sweep (K <= 16) with the log-likelihood of its input (P, Q) folded in."""
+    N, K = Q.shape
+    call("adx_em_sweep_loglik", G.data_ptr(), M, N, K, ADX_F64, P.data_ptr(), Q.data_ptr(),
+         workspace.data_ptr(), workspace.numel(), _stream(G.device))
+
+
+def em_loglik_from_sweep(workspace: torch.Tensor, M: int, N: int, K: int, out: torch.Tensor | None = None):
+    """The log-likelihood left by the last em_sweep_loglik in ``workspace`` (device float64)."""
+    out = torch.empty((), dtype=torch.float64, device=workspace.device) if out is None else out
+    call("adx_em_loglik_from_sweep", workspace.data_ptr(), workspace.numel(), M, N, K, ADX_F64, out.data_ptr(),
+         _stream(workspace.device))
+    return out
+
+
+def em_adam_update(P, Q, P32, Q32, mP, vP, mQ, vQ, q_bat, M, t, lr, beta1, beta2, eps, precision,
+                   workspace: torch.Tensor) -> None:
+    """EM targets + Adam move from the partial sums of the last sweep in ``workspace``."""
+    N, K = Q.shape
+    call("adx_em_adam_update", M, N, K, precision_code(precision), P.data_ptr(), Q.data_ptr(), _ptr(P32),
+         _ptr(Q32), mP.data_ptr(), vP.data_ptr(), mQ.data_ptr(), vQ.data_ptr(), q_bat.data_ptr(), float(t),
+         float(lr), float(beta1), float(beta2), float(eps), workspace.data_ptr(), workspace.numel(),
+         _stream(P.device))
+
+
 def em_targets(P, Q, A, B, T, q_bat, P_EM=None, Q_EM=None):
     M, K = P.shape
     N = Q.shape[0]

@@ -302,18 +302,36 @@ def time_steps(prec, G, P0, Q0, M_loc, N, K, dev, steps, warmup, sharded, clocks
     llp = "f64" if prec == "f64" else "f32"
     Pll, Qll = (P, Q) if llp == "f64" else (P32, Q32)
     launches = {"n": 0}
+    fold = {"need": True}
     if not sharded:
-        # kernels per fused iteration: sweep (+ the 16-bit copy of Q for the tensor-core
-        # sweep) and the update kernel; per check: the log-likelihood kernel and its final sum
         opt = EMAdamOptimizer(P.shape, Q.shape, HP["lr"], HP["beta1"], HP["beta2"], HP["eps"], dev, prec)
         per_iter = 3 if prec in TC_PRECISIONS else 2
+        if opt.can_fold_check(K):
+            # float64: as the optimiser runs it, the check after every 5th iteration is folded
+            # into the next iteration's sweep (kernels: the sweep, the partials' sum and the
+            # update, read back as the reference's .item()); other iterations are fused
 
-        def one_step(it):
-            opt.fused_iteration(G, P, Q, P32, Q32, M_loc, ws)
-            launches["n"] += per_iter
-            if (it + 1) % CHECK == 0:
-                float(ops.loglik_device(G, Pll, Qll, M_loc, llp).item())
-                launches["n"] += 2
+            def one_step(it):
+                if fold["need"]:
+                    float(opt.sweep_with_loglik(G, P, Q, M_loc, ws).item())
+                    opt.apply_update(P, Q, None, None, M_loc, ws)
+                    launches["n"] += 3
+                    fold["need"] = False
+                else:
+                    opt.fused_iteration(G, P, Q, P32, Q32, M_loc, ws)
+                    launches["n"] += 2
+                if (it + 1) % CHECK == 0:
+                    fold["need"] = True
+        else:
+            # kernels per fused iteration: sweep (+ the 16-bit copy of Q for the tensor-core
+            # sweep) and the update kernel; per check: the log-likelihood kernel and its final sum
+
+            def one_step(it):
+                opt.fused_iteration(G, P, Q, P32, Q32, M_loc, ws)
+                launches["n"] += per_iter
+                if (it + 1) % CHECK == 0:
+                    float(ops.loglik_device(G, Pll, Qll, M_loc, llp).item())
+                    launches["n"] += 2
     else:
         # SNP-sharded: local sweep + statistics, all-reduce of T, targets, Adam (Q replicated)
         run = ShardedAdamEM(G, P, Q, M_loc, K, HP["beta1"], HP["beta2"], HP["eps"], HP["lr"],
@@ -332,6 +350,9 @@ def time_steps(prec, G, P0, Q0, M_loc, N, K, dev, steps, warmup, sharded, clocks
         one_step(it)
     torch.cuda.synchronize()
     launches["n"] = 0
+    # folded checks: the timed steps hold a check every 5th step, the first at step 0 (the
+    # check due after the last warm-up step)
+    fold["need"] = True
     if sharded:
         torch.distributed.barrier()
     torch.cuda.synchronize()

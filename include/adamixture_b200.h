@@ -120,6 +120,23 @@ int adx_em_stats(const uint8_t* G, int64_t M, int64_t N, int K, int precision, c
 int adx_em_sweep(const uint8_t* G, int64_t M, int64_t N, int K, int precision, const void* P,
                  const void* Q, void* workspace, size_t workspace_bytes, void* stream);
 
+/* The E-step sweep of an iteration with the previous iteration's log-likelihood check folded
+ * in (float64, K <= 16; ADX_ERR_UNSUPPORTED otherwise): the reference checks
+ * loglikelihood_gpu(P, Q) after an Adam move (adamixture/model/em_adam_gpu.py:330-353) and the
+ * next E-step sweeps the same (P, Q), so this sweep leaves the partial sums of adx_em_sweep
+ * and the log-likelihood of its input, which adx_em_loglik_from_sweep sums into the device
+ * double *out (bit-identical to adx_loglik at ADX_F64). adx_em_adam_update then applies the
+ * EM targets and the Adam move from the workspace (the second half of adx_em_adam_iteration),
+ * after the caller has read the check and chosen the learning rate. */
+int adx_em_sweep_loglik(const uint8_t* G, int64_t M, int64_t N, int K, int precision, const void* P,
+                        const void* Q, void* workspace, size_t workspace_bytes, void* stream);
+int adx_em_loglik_from_sweep(void* workspace, size_t workspace_bytes, int64_t M, int64_t N, int K,
+                             int precision, double* out, void* stream);
+int adx_em_adam_update(int64_t M, int64_t N, int K, int precision, double* P, double* Q, float* P32,
+                       float* Q32, double* mP, double* vP, double* mQ, double* vQ, const double* q_bat,
+                       double t, double lr, double beta1, double beta2, double eps, void* workspace,
+                       size_t workspace_bytes, void* stream);
+
 /* EM targets from the statistics (em_final_update, em_adam_gpu.py:82-117):
  * P_EM = A P / max(P(A-B)+B, 1e-5); Q_EM = Q T / max(q_bat, 1e-5), rows / max(sum, 1e-5). */
 int adx_em_targets(const double* P, const double* Q, const double* A, const double* B,

@@ -320,3 +320,51 @@ def test_reference_op_names(ops, demo):
     G = dev_t(demo["packed"])
     out = torch.ops.pack2bit.unpack2bit_gpu_chunk_uint8(G, 100, 8192, M, 0, 512)
     assert np.array_equal(out.cpu().numpy(), orc.unpack(demo["packed"], M, 100, 8192))
+
+
+@pytest.mark.parametrize("name", ["demo", "synth"])
+def test_sweep_with_folded_check_equals_separate_check(ops, name, request):
+    # the float64 sweep that also returns the log-likelihood of its input: the check equals
+    # loglikelihood_gpu bit for bit, and its partial sums give the fused iteration's move
+    from adamixture_b200.model.em_adam_gpu import EMAdamOptimizer, loglikelihood_gpu
+
+    d = request.getfixturevalue(name)
+    M, N = int(d["M"]), int(d["N"])
+    G = dev_t(d["packed"])
+    runs = []
+    for folded in (True, False):
+        P, Q = dev_t(d["P0"]).clone(), dev_t(d["Q0"]).clone()
+        opt = EMAdamOptimizer(P.shape, Q.shape, 0.005, 0.80, 0.88, 1e-8, G.device, "f64")
+        ws = torch.zeros(ops.em_workspace_bytes(M, N, Q.shape[1], "f64"), dtype=torch.uint8, device=G.device)
+        checks = []
+        for it in range(7):
+            if folded and it % 3 == 0:
+                checks.append(float(opt.sweep_with_loglik(G, P, Q, M, ws).item()))
+                opt.apply_update(P, Q, None, None, M, ws)
+            else:
+                if not folded and it % 3 == 0:
+                    checks.append(loglikelihood_gpu(G, P, Q, M, N, 8192, G.device, 256))
+                opt.fused_iteration(G, P, Q, None, None, M, ws)
+        runs.append((P.cpu().numpy(), Q.cpu().numpy(), checks))
+    assert np.array_equal(runs[0][0], runs[1][0]) and np.array_equal(runs[0][1], runs[1][1])
+    assert runs[0][2] == runs[1][2], (runs[0][2], runs[1][2])
+
+
+@pytest.mark.parametrize("name", ["demo", "synth"])
+def test_optimiser_with_folded_checks_equals_the_reference_loop(ops, name, request):
+    # the float64 optimiser folds each check into the next sweep; the returned model, the
+    # check trace and the stop point equal those of the loop that checks after each move
+    from adamixture_b200.model.em_adam_gpu import _optimize_parameters_gpu_once
+
+    d = request.getfixturevalue(name)
+    M, N, K = int(d["M"]), int(d["N"]), int(d["K"])
+    G = dev_t(d["packed"])
+    out = []
+    for fold in (True, False):
+        tr = []
+        P, Q = _optimize_parameters_gpu_once(G, dev_t(d["P0"]).clone(), dev_t(d["Q0"]).clone(), 0.005, 0.80, 0.88,
+                                             1e-8, 10000, 5, K, M, N, 0.5, 1e-4, 3, 0.1, G.device, 8192, 512,
+                                             precision="f64", trace=tr, fold_checks=fold)
+        out.append((P.cpu().numpy(), Q.cpu().numpy(), [(it, L) for it, L, _ in tr]))
+    assert out[0][2] == out[1][2]
+    assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][1], out[1][1])

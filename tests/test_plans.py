@@ -104,16 +104,32 @@ def _batch_bytes(M, N, Ks):
     return _lib.query_size("adx_em_batch_workspace_bytes", M, N, len(Ks), ctypes.addressof(arr))
 
 
+def f64_plan(M, N):
+    """The float64 tensor-core sweep's partition (K <= 16), restated: 256-sample sub-tiles,
+    16-SNP chunks, splits x SNP blocks near 1776 blocks minimising partial traffic."""
+    import math
+
+    n_stile = cdiv(N, 256)
+    n_split = int(math.floor(math.sqrt(1776 * N / (2.0 * M)) + 0.5))
+    n_split = max(1, min(n_split, n_stile, 1776))
+    n_mblk = max(1, min(1776 // n_split, cdiv(M, 16)))
+    mb = cdiv(cdiv(M, n_mblk), 16) * 16
+    return n_split, cdiv(M, mb)
+
+
 @pytest.mark.parametrize("M,N", [(100_000, 20_000), (3_001, 4_096), (33, 1_000_000), (500_000, 200_000)])
 def test_batch_workspace_is_the_single_problem_partials_side_by_side(M, N):
     # the float64 plan does not depend on K, so a batch's workspace is a 256-byte header plus
-    # every problem's single-problem partials (each 256-byte aligned)
+    # every problem's single-problem partials (each 256-byte aligned); a single problem's
+    # workspace also holds one log-likelihood partial per block after its partials
+    n_split, n_mblk = f64_plan(M, N)
     Ks = [2, 7, 10, 12, 16, 1]
-    header = 256
-    total = header
+    total = 256
     for K in Ks:
+        part = cdiv((n_split * M * 2 * K + n_mblk * N * K) * 8, 256) * 256
         single = _lib.query_size("adx_em_workspace_bytes", M, N, K, _lib.ADX_F64)
-        total += cdiv(single - header, 256) * 256
+        assert single == 256 + part + n_split * n_mblk * 8, (M, N, K)
+        total += part
     assert _batch_bytes(M, N, Ks) == total
 
 
