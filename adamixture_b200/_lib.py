@@ -46,6 +46,8 @@ SIGNATURES: dict[str, list] = {
     "adx_em_batch_apply": [I64, I64, c_int, P, c_int, c_int, P, P, P, P, P, P, P, P, P, P, c_double,
                            c_double, c_double, c_double, c_double, P, c_size_t, P],
     "adx_em_sweep_loglik": [P, I64, I64, c_int, c_int, P, P, P, c_size_t, P],
+    "adx_em_sweep_blocks_info": [I64, I64, c_int, c_int, P, P, P],
+    "adx_em_sweep_blocks": [P, I64, I64, c_int, c_int, P, P, c_int, c_int, P, c_size_t, P],
     "adx_em_loglik_from_sweep": [P, c_size_t, I64, I64, c_int, c_int, P, P],
     "adx_em_adam_update": [I64, I64, c_int, c_int, P, P, P, P, P, P, P, P, P, c_double, c_double, c_double,
                            c_double, c_double, P, c_size_t, P],

@@ -400,7 +400,7 @@ int dmma_plan_width();
 int dmma_plan_chunk();
 int dmma_sweep(const uint8_t* G, const double* P, const double* Q, int64_t M, int64_t N, int K,
                int64_t n_stile, int n_split, int n_mblk, int64_t mb, double* ABp, double* Tp,
-               cudaStream_t st, double* llp = nullptr);
+               cudaStream_t st, double* llp = nullptr, int b0 = 0, int b1 = 0);
 // Float64 sweeps for K <= 16 run on the float64 tensor-core MMA (em_sweep_dmma.cu).
 constexpr int DMMA_MAX_K = 16;
 
@@ -766,6 +766,48 @@ extern "C" int adx_em_adam_update(int64_t M, int64_t N, int K, int precision, do
   if (workspace_bytes < pl.bytes()) { adx_set_message("adx_em_adam_update: workspace too small"); return ADX_ERR_WORKSPACE; }
   return em_update(pl, workspace, 1, nullptr, nullptr, nullptr, q_bat, P, Q, P32, Q32, mP, vP, mQ, vQ,
                    AdamArgs{t, lr, beta1, beta2, eps}, as_stream(stream));
+}
+
+// ---------------------------------------------------------------- block-range sweeps
+//
+// The float64 sweep (K <= 16) over a range of its SNP blocks, for callers that upload the
+// packed matrix in pieces and sweep each piece as it lands: the partition is the full
+// sweep's, each block's partial sums depend on that block alone, so the ranges of one
+// workspace add up to exactly the full sweep.
+
+extern "C" int adx_em_sweep_blocks_info(int64_t M, int64_t N, int K, int precision, int64_t* snps_per_block,
+                                        int* n_blocks, int* ctas_per_block) {
+  EmPlan pl;
+  const int rc = em_plan(M, N, K, precision, pl);
+  if (rc || !snps_per_block || !n_blocks || !ctas_per_block) { adx_set_message("adx_em_sweep_blocks_info: bad arguments"); return rc ? rc : ADX_ERR_ARG; }
+  if (precision != ADX_F64 || K > DMMA_MAX_K) {
+    adx_set_message("adx_em_sweep_blocks_info: float64 with K <= 16 only");
+    return ADX_ERR_UNSUPPORTED;
+  }
+  *snps_per_block = pl.mb;
+  *n_blocks = pl.n_mblk;
+  *ctas_per_block = pl.n_split;
+  return ADX_OK;
+}
+
+extern "C" int adx_em_sweep_blocks(const uint8_t* G, int64_t M, int64_t N, int K, int precision, const void* P,
+                                   const void* Q, int b0, int b1, void* workspace, size_t workspace_bytes,
+                                   void* stream) {
+  EmPlan pl;
+  int rc = em_plan(M, N, K, precision, pl);
+  if (rc) { adx_set_message("adx_em_sweep_blocks: bad shape or precision"); return rc; }
+  if (precision != ADX_F64 || K > DMMA_MAX_K) {
+    adx_set_message("adx_em_sweep_blocks: float64 with K <= 16 only");
+    return ADX_ERR_UNSUPPORTED;
+  }
+  if (!G || !P || !Q || !workspace || b0 < 0 || b1 > pl.n_mblk || b0 >= b1) {
+    adx_set_message("adx_em_sweep_blocks: bad arguments (0 <= b0 < b1 <= n_blocks)");
+    return ADX_ERR_ARG;
+  }
+  if (workspace_bytes < pl.bytes()) { adx_set_message("adx_em_sweep_blocks: workspace too small"); return ADX_ERR_WORKSPACE; }
+  double* ABp = reinterpret_cast<double*>(static_cast<uint8_t*>(workspace) + EmPlan::HEADER);
+  return dmma_sweep(G, (const double*)P, (const double*)Q, M, N, K, pl.n_stile, pl.n_split, pl.n_mblk, pl.mb, ABp,
+                    ABp + pl.ab_elems, as_stream(stream), nullptr, b0, b1);
 }
 
 // The float64 log-likelihood on the float64 MMA (em_sweep_dmma.cu) uses the float64 sweep's

@@ -107,6 +107,8 @@ struct Args {
   int n_split, n_mblk;
   int64_t mb;
   double* llp;        // the sweep with the log-likelihood: one partial per CTA
+  int mblk0 = 0;      // the launch covers SNP blocks [mblk0, mblk0 + nmb) (all: 0, n_mblk)
+  int nmb = 0;
 };
 
 // Split x = m * 2^e with m in [0.5, 1): returns m, adds e to e.
@@ -430,8 +432,8 @@ template <int KS, int MAXP, bool LL>
 __global__ void __launch_bounds__(TPB, 1) em_sweep_dmma_kernel(Args a, Probs<MAXP> ps) {
   static_assert(!LL || MAXP == 1, "the log-likelihood rides on single-problem sweeps");
   extern __shared__ __align__(16) double sm[];
-  const int mblk = blockIdx.x % a.n_mblk;
-  const int split = blockIdx.x / a.n_mblk;
+  const int mblk = a.mblk0 + (int)(blockIdx.x % a.nmb);
+  const int split = blockIdx.x / a.nmb;
   int chunk_no = 0;   // parity of the A/B reduction buffer
   double prod = 1.0;
   int ex = 0;
@@ -555,7 +557,7 @@ static int dmma_launch(const dm::Args& a, const dm::Probs<MAXP>& ps, cudaStream_
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dm::SMEM_BYTES));
     attr_set[dev] = true;
   }
-  dm::em_sweep_dmma_kernel<KS, MAXP, LL><<<(unsigned)(a.n_split * a.n_mblk), dm::TPB, dm::SMEM_BYTES, st>>>(a, ps);
+  dm::em_sweep_dmma_kernel<KS, MAXP, LL><<<(unsigned)(a.n_split * a.nmb), dm::TPB, dm::SMEM_BYTES, st>>>(a, ps);
   ADX_LAUNCH_CHECK();
   return ADX_OK;
 }
@@ -565,11 +567,16 @@ static int dmma_vec(const uint8_t* G, int64_t N) {
 }
 
 // llp != nullptr: the sweep also writes one log-likelihood partial of its input per CTA.
+// Blocks [b0, b1) of the partition only (b1 <= 0: all of them); llp needs all blocks.
 int dmma_sweep(const uint8_t* G, const double* P, const double* Q, int64_t M, int64_t N, int K,
                int64_t n_stile, int n_split, int n_mblk, int64_t mb, double* ABp, double* Tp,
-               cudaStream_t st, double* llp) {
+               cudaStream_t st, double* llp, int b0, int b1) {
   if (K < 1 || K > 16) return ADX_ERR_UNSUPPORTED;
-  const dm::Args a{M, N, n_stile, n_split, n_mblk, mb, llp};
+  if (b1 <= 0) { b0 = 0; b1 = n_mblk; }
+  if (b0 < 0 || b1 > n_mblk || b0 >= b1 || (llp && (b0 != 0 || b1 != n_mblk))) return ADX_ERR_ARG;
+  dm::Args a{M, N, n_stile, n_split, n_mblk, mb, llp};
+  a.mblk0 = b0;
+  a.nmb = b1 - b0;
   dm::Probs<1> ps;
   ps.p[0] = dm::Prob{G, P, Q, ABp, Tp, K, dmma_vec(G, N)};
   ps.n = 1;
@@ -589,7 +596,8 @@ int dmma_sweep_batch(int64_t M, int64_t N, int n, const int* K, const uint8_t* c
                      const double* const* Q, double* const* ABp, double* const* Tp, int64_t n_stile, int n_split,
                      int n_mblk, int64_t mb, cudaStream_t st) {
   if (n < 1 || n > DMMA_MAX_PROBLEMS) return ADX_ERR_ARG;
-  const dm::Args a{M, N, n_stile, n_split, n_mblk, mb, nullptr};
+  dm::Args a{M, N, n_stile, n_split, n_mblk, mb, nullptr};
+  a.nmb = n_mblk;
   dm::Probs<DMMA_MAX_PROBLEMS> ps;
   for (int p = 0; p < n; ++p) {
     if (K[p] < 1 || K[p] > 16 || !G[p]) return ADX_ERR_ARG;

@@ -327,16 +327,109 @@ def _loop_folded_checks(G, P, Q, M, N, K, opt, ws, max_iter, check, lr_decay, mi
     return state["P_best"], state["Q_best"]
 
 
+MAX_UPLOAD_PIECES = 4
+
+
+def upload_pieces(n_blocks: int, ctas_per_block: int, sms: int, max_pieces: int = MAX_UPLOAD_PIECES):
+    """Block ranges of the pieces in which a host matrix is uploaded and swept.
+
+    Each piece's sweep is one launch of ``ctas_per_block`` CTAs per block, one CTA per SM,
+    so a launch takes as long as its CTA count rounded up to whole waves of ``sms``. The
+    pieces are the most (up to ``max_pieces``) whose waves add up to the full sweep's, the
+    larger ones last: piece i gets w_i waves and the blocks that fit in them. More pieces
+    let the sweep start sooner after the upload starts; a piece that would leave part of a
+    wave idle would make the sweeps slower than the full sweep. Returns [(b0, b1), ...]."""
+    waves = -(-n_blocks * ctas_per_block // sms)
+    for q in range(min(max_pieces, waves, n_blocks), 1, -1):
+        w = [waves // q + (1 if i >= q - waves % q else 0) for i in range(q)]
+        fit = [wi * sms // ctas_per_block for wi in w]
+        if min(fit) < 1 or sum(fit) < n_blocks:
+            continue
+        out, b = [], 0
+        for f in fit:
+            if b < n_blocks:
+                out.append((b, min(n_blocks, b + f)))
+                b += f
+        return out
+    return [(0, n_blocks)]
+
+
+def _upload_and_prime(G_host, P, Q, M, K, opt, device):
+    """Copy the packed matrix from host memory to ``device`` in pieces of whole SNP blocks
+    (``upload_pieces``) on a copy stream and run the priming iteration's float64 sweep and
+    sample counts on each piece as it lands, then the priming move: the copy overlaps the
+    sweep. The partial sums are the full sweep's, so the primed (P, Q) equal those of
+    uploading first and priming after. Returns the device matrix and the workspace."""
+    N = Q.shape[0]
+    G = torch.empty(G_host.shape, dtype=torch.uint8, device=device)
+    ws = ops.Workspace.get(G.device, ops.em_workspace_bytes(M, N, K, "f64"))
+    spb, nb, cpb = ops.em_sweep_blocks_info(M, N, K)
+    sms = torch.cuda.get_device_properties(G.device).multi_processor_count
+    rows_pb = spb // 4                                  # packed rows per block
+    main = torch.cuda.current_stream(G.device)
+    copy = torch.cuda.Stream(G.device)
+    copy.wait_stream(main)
+    q = torch.zeros(N, dtype=torch.float64, device=G.device)
+    rows = G.shape[0]
+    pieces = []
+    with torch.cuda.stream(copy):
+        for b0, b1 in upload_pieces(nb, cpb, sms):
+            r0, r1 = b0 * rows_pb, min(rows, b1 * rows_pb)
+            G[r0:r1].copy_(G_host[r0:r1], non_blocking=True)
+            ev = torch.cuda.Event()
+            ev.record(copy)
+            pieces.append((b0, b1, r0, r1, ev))
+    for b0, b1, r0, r1, ev in pieces:
+        main.wait_event(ev)
+        ops.em_sweep_blocks(G, P, Q, M, b0, b1, ws)
+        # per-sample observed counts of the piece's SNPs (exact integers: any order)
+        q += ops.sample_counts(G[r0:r1], min(M, 4 * r1) - 4 * r0)
+    G.record_stream(copy)
+    opt.q_bat.copy_(q)
+    opt._qbat_key = (G.data_ptr(), tuple(G.shape), M)
+    opt.apply_update(P, Q, None, None, M, ws)
+    return G, ws
+
+
 def optimize_parameters_gpu(G, P, Q, lr, beta1, beta2, reg_adam, max_iter, check, K, M, N,
                             lr_decay, min_lr, patience, tol_adam, device, chunk_size,
                             threads_per_block, precision=None, trace=None):
     """Adam-EM on the GPU (em_adam_gpu.py:359-385). The reference's OOM retry halves the
     chunk size; the fused sweep has no per-chunk temporaries, so there is nothing to
-    retry: the only allocations are P/Q-sized buffers and the partial-sum workspace."""
+    retry: the only allocations are P/Q-sized buffers and the partial-sum workspace.
+
+    ``G`` may also be a packed matrix in (pinned) host memory, with P and Q on the host or
+    the device: in float64 with K <= 16 it is then uploaded to ``device`` in pieces, each
+    piece swept by the priming iteration as it lands (the copy overlaps the sweep); the
+    iterations are the same as for a resident matrix."""
+    if not G.is_cuda:
+        dev = torch.device(device)
+        if dev.type != "cuda":
+            raise ValueError("adamixture_b200 runs on CUDA devices only (got a CPU device)")
+        P = P.to(dev, torch.float64).contiguous().clone()
+        Q = Q.to(dev, torch.float64).contiguous().clone()
+        opt_prec = resolve_precision(K, precision)
+        if opt_prec == "f64" and K <= 16 and (precision or _PRECISION) != "mixed":
+            return _optimize_streamed(G, P, Q, lr, beta1, beta2, reg_adam, max_iter, check, K, M, N, lr_decay,
+                                      min_lr, patience, tol_adam, dev, trace)
+        G = G.to(dev)
     _require_cuda(G, P, Q)
     P = P.to(torch.float64).contiguous().clone()
     Q = Q.to(torch.float64).contiguous().clone()
     return _optimize_parameters_gpu_once(G, P, Q, lr, beta1, beta2, reg_adam, max_iter, check, K,
                                          M, N, lr_decay, min_lr, patience, tol_adam, device,
                                          chunk_size, threads_per_block, precision, trace)
+
+
+def _optimize_streamed(G_host, P, Q, lr, beta1, beta2, reg_adam, max_iter, check, K, M, N, lr_decay, min_lr,
+                       patience, tol_adam, device, trace):
+    """``optimize_parameters_gpu`` from a host matrix, float64: the upload overlaps the
+    priming sweep, then the reference loop with folded checks."""
+    opt = EMAdamOptimizer(P.shape, Q.shape, lr, beta1, beta2, reg_adam, device, "f64")
+    ts = time.time()
+    t_start = time.perf_counter()
+    G, ws = _upload_and_prime(G_host, P, Q, M, K, opt, device)
+    log.info(f"    Performed priming iteration... ({time.time() - ts:.1f}s)\n")
+    return _loop_folded_checks(G, P, Q, M, N, K, opt, ws, max_iter, check, lr_decay, min_lr, patience, tol_adam,
+                               trace, t_start)
 

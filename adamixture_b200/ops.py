@@ -210,6 +210,30 @@ def em_sweep_loglik(G: torch.Tensor, P: torch.Tensor, Q: torch.Tensor, M: int, w
          workspace.data_ptr(), workspace.numel(), _stream(G.device))
 
 
+def em_sweep_blocks_info(M: int, N: int, K: int) -> tuple[int, int, int]:
+    """(SNPs per block, number of blocks, CTAs per block) of the float64 sweep's partition
+    (K <= 16); each CTA occupies one SM."""
+    import ctypes
+
+    spb, nb, cpb = ctypes.c_int64(0), ctypes.c_int(0), ctypes.c_int(0)
+    call("adx_em_sweep_blocks_info", M, N, K, ADX_F64, ctypes.addressof(spb), ctypes.addressof(nb),
+         ctypes.addressof(cpb))
+    return int(spb.value), int(nb.value), int(cpb.value)
+
+
+def em_sweep_blocks(G: torch.Tensor, P: torch.Tensor, Q: torch.Tensor, M: int, b0: int, b1: int,
+                    workspace: torch.Tensor) -> None:
+    """The float64 sweep over SNP blocks [b0, b1) into ``workspace``'s partials: only the
+    packed rows of those blocks are read, and the ranges of one workspace add up to exactly
+    the full sweep (``em_sweep``)."""
+    _check(G, "G", torch.uint8)
+    _check(P, "P", torch.float64, G.device)
+    _check(Q, "Q", torch.float64, G.device)
+    N, K = Q.shape
+    call("adx_em_sweep_blocks", G.data_ptr(), M, N, K, ADX_F64, P.data_ptr(), Q.data_ptr(), int(b0), int(b1),
+         workspace.data_ptr(), workspace.numel(), _stream(G.device))
+
+
 def em_loglik_from_sweep(workspace: torch.Tensor, M: int, N: int, K: int, out: torch.Tensor | None = None):
     """The log-likelihood left by the last em_sweep_loglik in ``workspace`` (device float64)."""
     out = torch.empty((), dtype=torch.float64, device=workspace.device) if out is None else out

@@ -137,6 +137,19 @@ int adx_em_adam_update(int64_t M, int64_t N, int K, int precision, double* P, do
                        double t, double lr, double beta1, double beta2, double eps, void* workspace,
                        size_t workspace_bytes, void* stream);
 
+/* The float64 sweep (K <= 16) over SNP blocks [b0, b1) of its partition only, into the same
+ * workspace partials: blocks are independent, so ranges that cover 0..n_blocks add up to
+ * exactly adx_em_sweep. For callers that upload the packed matrix in pieces and sweep each
+ * piece as it lands (block b holds SNPs [b*snps_per_block, (b+1)*snps_per_block), a multiple
+ * of 16; each block is *ctas_per_block CTAs of one SM each, so a range fills whole waves
+ * when its CTA count is a multiple of the SM count). No counterpart in the reference (it
+ * sweeps fixed 8192-SNP chunks of a resident matrix, adamixture/model/em_adam_gpu.py:187-197). */
+int adx_em_sweep_blocks_info(int64_t M, int64_t N, int K, int precision, int64_t* snps_per_block,
+                             int* n_blocks, int* ctas_per_block);
+int adx_em_sweep_blocks(const uint8_t* G, int64_t M, int64_t N, int K, int precision, const void* P,
+                        const void* Q, int b0, int b1, void* workspace, size_t workspace_bytes,
+                        void* stream);
+
 /* EM targets from the statistics (em_final_update, em_adam_gpu.py:82-117):
  * P_EM = A P / max(P(A-B)+B, 1e-5); Q_EM = Q T / max(q_bat, 1e-5), rows / max(sum, 1e-5). */
 int adx_em_targets(const double* P, const double* Q, const double* A, const double* B,

@@ -368,3 +368,58 @@ def test_optimiser_with_folded_checks_equals_the_reference_loop(ops, name, reque
         out.append((P.cpu().numpy(), Q.cpu().numpy(), [(it, L) for it, L, _ in tr]))
     assert out[0][2] == out[1][2]
     assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][1], out[1][1])
+
+
+def _ranges(nb):
+    """An irregular cover of [0, nb) by consecutive block ranges."""
+    cuts = sorted(c for c in {0, 1, nb // 3, 2 * nb // 3 + 1, nb} if c <= nb)
+    return [(a, b) for a, b in zip(cuts, cuts[1:]) if a < b]
+
+
+@pytest.mark.parametrize("N,M,K", [(105, 1000, 3), (2000, 9001, 7), (777, 40_003, 16), (3000, 5, 2)])
+def test_block_range_sweeps_equal_the_full_sweep(ops, N, M, K):
+    # the float64 sweep over ranges of its SNP blocks, each reading only its own packed rows:
+    # the ranges of one workspace add up to the full sweep's workspace bit for bit
+    rng = np.random.default_rng(N + M + K)
+    g = rng.integers(0, 3, size=(M, N), dtype=np.uint8)
+    g[rng.random((M, N)) < 0.02] = 3
+    G = dev_t(orc.pack(g))
+    P = dev_t(np.clip(rng.random((M, K)), 1e-5, 1 - 1e-5))
+    Q = rng.random((N, K))
+    Q = dev_t(Q / Q.sum(1, keepdims=True))
+    spb, nb, cpb = ops.em_sweep_blocks_info(M, N, K)
+    assert spb % 16 == 0 and nb == -(-M // spb) and cpb * nb <= 1776
+    nbytes = ops.em_workspace_bytes(M, N, K, "f64")
+    full = torch.zeros(nbytes, dtype=torch.uint8, device=G.device)
+    ops.em_sweep(G, P, Q, M, "f64", full)
+    parts = torch.zeros_like(full)
+    Gp = torch.full_like(G, 0xFF)        # rows outside the swept ranges hold junk (all missing)
+    for b0, b1 in reversed(_ranges(nb)):
+        r0, r1 = b0 * spb // 4, min(G.shape[0], b1 * spb // 4)
+        Gp[r0:r1] = G[r0:r1]
+        ops.em_sweep_blocks(Gp, P, Q, M, b0, b1, parts)
+    assert torch.equal(full, parts)
+    with pytest.raises(Exception, match="b0 < b1"):
+        ops.em_sweep_blocks(G, P, Q, M, 0, nb + 1, parts)
+
+
+@pytest.mark.parametrize("name", ["demo", "synth"])
+def test_optimiser_from_host_matrix_equals_resident(ops, name, request, monkeypatch):
+    # a packed matrix in pinned host memory is uploaded in pieces that the priming sweep
+    # consumes as they land; the fit equals the one from the device-resident matrix exactly
+    from adamixture_b200.model import em_adam_gpu as em
+
+    d = request.getfixturevalue(name)
+    M, N, K = int(d["M"]), int(d["N"]), int(d["K"])
+    monkeypatch.setattr(em, "upload_pieces", lambda nb, cpb, sms: _ranges(nb))   # several pieces
+    out = []
+    for host in (True, False):
+        G = torch.from_numpy(d["packed"]).pin_memory() if host else dev_t(d["packed"])
+        P0 = torch.from_numpy(d["P0"]) if host else dev_t(d["P0"])
+        Q0 = torch.from_numpy(d["Q0"]) if host else dev_t(d["Q0"])
+        tr = []
+        P, Q = em.optimize_parameters_gpu(G, P0, Q0, 0.005, 0.80, 0.88, 1e-8, 60, 5, K, M, N, 0.5, 1e-4, 3, 0.1,
+                                          torch.device("cuda", 0), 8192, 512, precision="f64", trace=tr)
+        out.append((P.cpu().numpy(), Q.cpu().numpy(), [(it, L) for it, L, _ in tr]))
+    assert out[0][2] == out[1][2]
+    assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][1], out[1][1])
