@@ -41,6 +41,11 @@ SIGNATURES: dict[str, list] = {
                       c_double, c_double, P, P, P],
     "adx_em_adam_iteration": [P, I64, I64, c_int, c_int, P, P, P, P, P, P, P, P, P, c_double,
                               c_double, c_double, c_double, c_double, P, c_size_t, P],
+    "adx_em_graph_create": [P, I64, I64, c_int, c_int, P, P, P, P, P, P, P, P, P, c_int, c_double, c_double,
+                            c_double, c_double, P, P, c_size_t, P],
+    "adx_em_graph_launch": [P, c_double, P],
+    "adx_em_graph_iterations": [P, P],
+    "adx_em_graph_destroy": [P],
     "adx_em_batch_workspace_bytes": [I64, I64, c_int, P, P],
     "adx_em_sweep_batch": [I64, I64, c_int, P, P, P, P, P, c_size_t, P],
     "adx_em_batch_apply": [I64, I64, c_int, P, c_int, c_int, P, P, P, P, P, P, P, P, P, P, c_double,

@@ -262,7 +262,11 @@ em_sweep_kernel(const uint8_t* __restrict__ G, const R* __restrict__ P, const R*
 
 struct AdamArgs {
   double t, lr, b1, b2, eps;
+  // captured iterations: the step is *t_dev + t (t the iteration's offset in the replay)
+  const double* t_dev = nullptr;
 };
+
+__device__ __forceinline__ double adam_step_no(const AdamArgs& ad) { return ad.t_dev ? *ad.t_dev + ad.t : ad.t; }
 
 // mode 0: write A, B, T (float64 statistics). mode 1: EM targets + Adam move on P and Q.
 template <typename R, int KMAX>
@@ -276,8 +280,9 @@ __global__ void em_update_kernel(const R* __restrict__ ABp, const R* __restrict_
                                  double* __restrict__ mQ, double* __restrict__ vQ, AdamArgs ad) {
   const int64_t row = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (row >= M + N) return;
-  const double bc1 = 1.0 - pow(ad.b1, ad.t);
-  const double bc2 = 1.0 - pow(ad.b2, ad.t);
+  const double t = adam_step_no(ad);
+  const double bc1 = 1.0 - pow(ad.b1, t);
+  const double bc2 = 1.0 - pow(ad.b2, t);
   if (row < M) {
     const int64_t j = row;
     double A[KMAX], B[KMAX];
@@ -556,8 +561,9 @@ __global__ void adam_step_kernel(double* __restrict__ P, double* __restrict__ Q,
                                  float* __restrict__ Q32) {
   const int64_t row = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (row >= M + N) return;
-  const double bc1 = 1.0 - pow(ad.b1, ad.t);
-  const double bc2 = 1.0 - pow(ad.b2, ad.t);
+  const double t = adam_step_no(ad);
+  const double bc1 = 1.0 - pow(ad.b1, t);
+  const double bc2 = 1.0 - pow(ad.b2, t);
   const bool isP = row < M;
   const int64_t r = isP ? row : row - M;
   double* X = isP ? P : Q;
@@ -684,6 +690,110 @@ extern "C" int adx_em_adam_iteration(const uint8_t* G, int64_t M, int64_t N, int
   if (rc) return rc;
   return em_update(pl, workspace, 1, nullptr, nullptr, nullptr, q_bat, P, Q, P32, Q32, mP, vP, mQ,
                    vQ, AdamArgs{t, lr, beta1, beta2, eps}, st);
+}
+
+// ---------------------------------------------------------------- captured iterations
+//
+// n fused Adam-EM iterations (adx_em_adam_iteration) captured once into a CUDA graph and
+// replayed with one launch: 2n kernel launches and their host-side cost become one graph
+// launch, which matters when an iteration takes tens of microseconds (small cohorts). The
+// Adam step of the replay's iteration i (1..n) is *step_counter + i; adx_em_graph_launch
+// first sets the counter to the steps already taken, so a replay computes exactly the n
+// eager iterations t0+1..t0+n. Pointers, shapes and the learning rate are fixed at capture;
+// the caller keeps every buffer alive, at the same address, for the graph's lifetime.
+
+namespace adx {
+__global__ void set_counter_kernel(double* c, double v) { *c = v; }
+}  // namespace adx
+
+struct AdxEmGraph {
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  double* counter = nullptr;
+  int n = 0;
+};
+
+extern "C" int adx_em_graph_create(const uint8_t* G, int64_t M, int64_t N, int K, int precision, double* P,
+                                   double* Q, float* P32, float* Q32, double* mP, double* vP, double* mQ,
+                                   double* vQ, const double* q_bat, int n_iters, double lr, double beta1,
+                                   double beta2, double eps, double* step_counter, void* workspace,
+                                   size_t workspace_bytes, void** graph) {
+  EmPlan pl;
+  int rc = em_plan(M, N, K, precision, pl);
+  if (rc) { adx_set_message("adx_em_graph_create: bad shape or precision"); return rc; }
+  if (!G || !P || !Q || !mP || !vP || !mQ || !vQ || !q_bat || !workspace || !step_counter || !graph ||
+      n_iters < 1 || n_iters > 4096) {
+    adx_set_message("adx_em_graph_create: bad arguments (1 <= n_iters <= 4096, non-null buffers)");
+    return ADX_ERR_ARG;
+  }
+  if (precision != ADX_F64 && (!P32 || !Q32)) { adx_set_message("adx_em_graph_create: P32/Q32 required"); return ADX_ERR_ARG; }
+  if (workspace_bytes < pl.bytes()) { adx_set_message("adx_em_graph_create: workspace too small"); return ADX_ERR_WORKSPACE; }
+  *graph = nullptr;
+  const void* Pin = precision == ADX_F64 ? (const void*)P : (const void*)P32;
+  const void* Qin = precision == ADX_F64 ? (const void*)Q : (const void*)Q32;
+  // capture on a private stream (the caller's may be the legacy default stream, which cannot
+  // be captured); relaxed mode, so a kernel's first-use attribute setup may run inside
+  cudaStream_t cs = nullptr;
+  ADX_CUDA_TRY(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+  cudaError_t ce = cudaStreamBeginCapture(cs, cudaStreamCaptureModeRelaxed);
+  if (ce != cudaSuccess) {
+    cudaStreamDestroy(cs);
+    adx_set_cuda_error(ce);
+    return ADX_ERR_CUDA;
+  }
+  for (int i = 1; i <= n_iters && !rc; ++i) {
+    rc = em_sweep(pl, G, Pin, Qin, workspace, cs);
+    if (!rc)
+      rc = em_update(pl, workspace, 1, nullptr, nullptr, nullptr, q_bat, P, Q, P32, Q32, mP, vP, mQ, vQ,
+                     AdamArgs{(double)i, lr, beta1, beta2, eps, step_counter}, cs);
+  }
+  cudaGraph_t g = nullptr;
+  ce = cudaStreamEndCapture(cs, &g);
+  cudaStreamDestroy(cs);
+  if (rc || ce != cudaSuccess || !g) {
+    if (g) cudaGraphDestroy(g);
+    if (!rc) {
+      adx_set_cuda_error(ce != cudaSuccess ? ce : cudaErrorStreamCaptureInvalidated);
+      rc = ADX_ERR_CUDA;
+    }
+    cudaGetLastError();
+    return rc;
+  }
+  cudaGraphExec_t ex = nullptr;
+  ce = cudaGraphInstantiate(&ex, g, 0ULL);
+  if (ce != cudaSuccess) {
+    cudaGraphDestroy(g);
+    adx_set_cuda_error(ce);
+    return ADX_ERR_CUDA;
+  }
+  *graph = new AdxEmGraph{g, ex, step_counter, n_iters};
+  return ADX_OK;
+}
+
+extern "C" int adx_em_graph_launch(void* graph, double t0, void* stream) {
+  auto* h = static_cast<AdxEmGraph*>(graph);
+  if (!h || t0 < 0) { adx_set_message("adx_em_graph_launch: bad arguments"); return ADX_ERR_ARG; }
+  cudaStream_t st = as_stream(stream);
+  adx::set_counter_kernel<<<1, 1, 0, st>>>(h->counter, t0);
+  ADX_LAUNCH_CHECK();
+  ADX_CUDA_TRY(cudaGraphLaunch(h->exec, st));
+  return ADX_OK;
+}
+
+extern "C" int adx_em_graph_iterations(void* graph, int* n_iters) {
+  auto* h = static_cast<AdxEmGraph*>(graph);
+  if (!h || !n_iters) { adx_set_message("adx_em_graph_iterations: bad arguments"); return ADX_ERR_ARG; }
+  *n_iters = h->n;
+  return ADX_OK;
+}
+
+extern "C" int adx_em_graph_destroy(void* graph) {
+  auto* h = static_cast<AdxEmGraph*>(graph);
+  if (!h) return ADX_OK;
+  if (h->exec) cudaGraphExecDestroy(h->exec);
+  if (h->graph) cudaGraphDestroy(h->graph);
+  delete h;
+  return ADX_OK;
 }
 
 // ---------------------------------------------------------------- sweep + log-likelihood

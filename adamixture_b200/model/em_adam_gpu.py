@@ -33,6 +33,8 @@ from .. import ops
 log = logging.getLogger(__name__)
 
 _PRECISION = os.environ.get("ADX_PRECISION", "auto")
+# runs of fused iterations between log-likelihood checks replay a captured CUDA graph
+USE_GRAPHS = os.environ.get("ADX_GRAPHS", "1") != "0"
 
 
 def set_precision(p: str) -> None:
@@ -165,6 +167,42 @@ class EMAdamOptimizer:
                               self.reg_adam, self.precision, workspace)
 
 
+class _IterationGraphs:
+    """Runs of fused Adam-EM iterations (between two log-likelihood checks) as replays of a
+    captured CUDA graph (``ops.EmGraph``), one graph per (run length, learning rate,
+    arithmetic), built on first use; the replays equal the eager iterations bit for bit.
+    A run of one iteration, or ``enabled=False``, runs eagerly. ``ws`` must be a workspace of
+    the optimiser's own (``ops.em_workspace``)."""
+
+    def __init__(self, opt, G, P, Q, P32, Q32, M, ws, enabled=None):
+        self.opt, self.G, self.P, self.Q, self.P32, self.Q32, self.M, self.ws = opt, G, P, Q, P32, Q32, M, ws
+        self.enabled = USE_GRAPHS if enabled is None else enabled
+        self.cache = {}
+
+    def run(self, n: int) -> None:
+        opt = self.opt
+        if n <= 0:
+            return
+        if not self.enabled or n < 2:
+            for _ in range(n):
+                opt.fused_iteration(self.G, self.P, self.Q, self.P32, self.Q32, self.M, self.ws)
+            return
+        key = (n, opt.lr, opt.precision, self.ws.data_ptr())
+        g = self.cache.get(key)
+        if g is None:
+            q_bat = opt._sample_counts(self.G, self.M)
+            g = ops.EmGraph(self.G, self.P, self.Q, self.P32, self.Q32, opt.m_P, opt.v_P, opt.m_Q, opt.v_Q, q_bat,
+                            self.M, n, opt.lr, opt.beta1, opt.beta2, opt.reg_adam, opt.precision, self.ws)
+            self.cache[key] = g
+        g.launch(opt._t)
+        opt._t += n
+
+    def close(self) -> None:
+        for g in self.cache.values():
+            g.close()
+        self.cache.clear()
+
+
 def logl_batch_math(g_chunk, p_batch, Q):
     """Reference per-chunk log-likelihood in float64 torch (em_adam_gpu.py:226-248); kept
     for API compatibility; the library computes the sum with ``loglikelihood_gpu``."""
@@ -205,7 +243,7 @@ def _optimize_parameters_gpu_once(G, P, Q, lr, beta1, beta2, reg_adam, max_iter,
     dt = ops.input_dtype(prec)
     P32 = P.to(torch.float32).contiguous() if dt == torch.float32 else None
     Q32 = Q.to(torch.float32).contiguous() if dt == torch.float32 else None
-    ws = ops.Workspace.get(G.device, ops.em_workspace_bytes(M, N, K, prec))
+    ws = ops.em_workspace(M, N, K, prec, G.device)
 
     def loglik():
         if ll_prec == "f64":
@@ -228,13 +266,20 @@ def _optimize_parameters_gpu_once(G, P, Q, lr, beta1, beta2, reg_adam, max_iter,
     P_best, Q_best = P.clone(), Q.clone()
     wait_lr = 0
     ts = time.time()
-    for it in range(max_iter):
-        opt.fused_iteration(G, P, Q, P32, Q32, M, ws)
-        if (it + 1) % check == 0:
+    graphs = _IterationGraphs(opt, G, P, Q, P32, Q32, M, ws)
+    it = 0   # iterations done
+    try:
+        while it < max_iter:
+            # the fused iterations up to the next check (or the end), replayed from a graph
+            n = min(check - it % check, max_iter - it)
+            graphs.run(n)
+            it += n
+            if it % check:
+                continue
             L_cur = loglik()
             if trace is not None:
-                trace.append((it + 1, L_cur, time.perf_counter() - t_start))
-            log.info(f"    Iteration {it+1}, Log-likelihood: {L_cur:.1f}, Time: {time.time() - ts:.3f}s")
+                trace.append((it, L_cur, time.perf_counter() - t_start))
+            log.info(f"    Iteration {it}, Log-likelihood: {L_cur:.1f}, Time: {time.time() - ts:.3f}s")
             ts = time.time()
             if L_cur > L_best + tol_adam:
                 L_best = L_cur
@@ -247,7 +292,7 @@ def _optimize_parameters_gpu_once(G, P, Q, lr, beta1, beta2, reg_adam, max_iter,
                     # mixed precision: the first plateau ends the tensor-core phase; the same Adam
                     # state continues with float32 sweeps (same float32 P/Q shadows)
                     prec = opt.precision = "f32"
-                    ws = ops.Workspace.get(G.device, ops.em_workspace_bytes(M, N, K, prec))
+                    ws = graphs.ws = ops.em_workspace(M, N, K, prec, G.device)
                     log.info("    Plateau in the tensor-core phase: continuing with float32 E-steps.")
                     wait_lr = 0
                     continue
@@ -260,6 +305,8 @@ def _optimize_parameters_gpu_once(G, P, Q, lr, beta1, beta2, reg_adam, max_iter,
                         log.info("        Convergence reached.")
                         break
                     wait_lr = 0
+    finally:
+        graphs.close()
     log.info(f"\n    Final log-likelihood: {L_best:.1f}")
     return P_best, Q_best
 
@@ -309,18 +356,27 @@ def _loop_folded_checks(G, P, Q, M, N, K, opt, ws, max_iter, check, lr_decay, mi
 
     need = True   # the next sweep's input needs its log-likelihood (first: the primed point)
     stopped = False
-    for it in range(max_iter):
-        if need:
-            L = float(opt.sweep_with_loglik(G, P, Q, M, ws).item())
-            if not decide(L, it):
-                stopped = True
-                break
-            opt.apply_update(P, Q, None, None, M, ws)
-            need = False
-        else:
-            opt.fused_iteration(G, P, Q, None, None, M, ws)
-        if (it + 1) % check == 0:
-            need = True
+    graphs = _IterationGraphs(opt, G, P, Q, None, None, M, ws)
+    it = 0        # iterations done
+    try:
+        while it < max_iter:
+            if need:
+                L = float(opt.sweep_with_loglik(G, P, Q, M, ws).item())
+                if not decide(L, it):
+                    stopped = True
+                    break
+                opt.apply_update(P, Q, None, None, M, ws)
+                need = False
+                it += 1
+            else:
+                # the plain iterations up to the next check (or the end), replayed from a graph
+                n = min(check - it % check, max_iter - it)
+                graphs.run(n)
+                it += n
+            if it % check == 0:
+                need = True
+    finally:
+        graphs.close()
     if need and not stopped:
         decide(float(ops.loglik_device(G, P, Q, M, "f64").item()), max_iter)
     log.info(f"\n    Final log-likelihood: {state['L_best']:.1f}")
@@ -362,7 +418,7 @@ def _upload_and_prime(G_host, P, Q, M, K, opt, device):
     uploading first and priming after. Returns the device matrix and the workspace."""
     N = Q.shape[0]
     G = torch.empty(G_host.shape, dtype=torch.uint8, device=device)
-    ws = ops.Workspace.get(G.device, ops.em_workspace_bytes(M, N, K, "f64"))
+    ws = ops.em_workspace(M, N, K, "f64", G.device)
     spb, nb, cpb = ops.em_sweep_blocks_info(M, N, K)
     sms = torch.cuda.get_device_properties(G.device).multi_processor_count
     rows_pb = spb // 4                                  # packed rows per block

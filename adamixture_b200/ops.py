@@ -156,6 +156,12 @@ def em_workspace_bytes(M: int, N: int, K: int, precision) -> int:
     return query_size("adx_em_workspace_bytes", M, N, K, precision_code(precision))
 
 
+def em_workspace(M: int, N: int, K: int, precision, device) -> torch.Tensor:
+    """A zeroed E-step workspace of its own (not the shared cache): for callers that keep
+    its address, e.g. in a captured graph (``EmGraph``)."""
+    return torch.zeros(max(em_workspace_bytes(M, N, K, precision), 256), dtype=torch.uint8, device=device)
+
+
 def em_stats(G: torch.Tensor, P: torch.Tensor, Q: torch.Tensor, M: int, precision="f64"):
     """Sufficient statistics (A, B, T) of one E-step sweep, float64."""
     pc = precision_code(precision)
@@ -286,6 +292,56 @@ def em_adam_iteration(G, P, Q, P32, Q32, mP, vP, mQ, vQ, q_bat, M, t, lr, beta1,
          _ptr(P32), _ptr(Q32), mP.data_ptr(), vP.data_ptr(), mQ.data_ptr(), vQ.data_ptr(),
          q_bat.data_ptr(), float(t), float(lr), float(beta1), float(beta2), float(eps),
          ws.data_ptr(), ws.numel(), _stream(dev))
+
+
+class EmGraph:
+    """``n_iters`` fused Adam-EM iterations (``em_adam_iteration``) captured into one CUDA
+    graph by the library. ``launch(t0)`` replays them as steps t0+1 .. t0+n_iters, bit for
+    bit the eager iterations. The graph keeps a reference to every tensor it was captured
+    with (they must keep their storage: no resizing or reassignment of the buffers), and
+    ``workspace`` must be a buffer of its own, not the shared ``Workspace`` cache, which
+    may be reallocated."""
+
+    def __init__(self, G, P, Q, P32, Q32, mP, vP, mQ, vQ, q_bat, M, n_iters, lr, beta1, beta2, eps, precision,
+                 workspace: torch.Tensor):
+        import ctypes
+
+        pc = precision_code(precision)
+        N, K = Q.shape
+        dev = G.device
+        _check(G, "G", torch.uint8)
+        for x, n in ((P, "P"), (Q, "Q"), (mP, "m_P"), (vP, "v_P"), (mQ, "m_Q"), (vQ, "v_Q"), (q_bat, "q_bat")):
+            _check(x, n, torch.float64, dev)
+        if workspace.numel() < em_workspace_bytes(M, N, K, pc):
+            raise ValueError("EmGraph: workspace too small")
+        self.counter = torch.zeros(1, dtype=torch.float64, device=dev)
+        self._keep = (G, P, Q, P32, Q32, mP, vP, mQ, vQ, q_bat, workspace)
+        self.n_iters, self.lr, self.device = int(n_iters), float(lr), dev
+        h = ctypes.c_void_p(0)
+        call("adx_em_graph_create", G.data_ptr(), M, N, K, pc, P.data_ptr(), Q.data_ptr(), _ptr(P32), _ptr(Q32),
+             mP.data_ptr(), vP.data_ptr(), mQ.data_ptr(), vQ.data_ptr(), q_bat.data_ptr(), self.n_iters,
+             self.lr, float(beta1), float(beta2), float(eps), self.counter.data_ptr(), workspace.data_ptr(),
+             workspace.numel(), ctypes.addressof(h))
+        self._h = h.value
+
+    def launch(self, t0: int) -> None:
+        if not self._h:
+            raise RuntimeError("EmGraph: launched after close()")
+        call("adx_em_graph_launch", self._h, float(t0), _stream(self.device))
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            from ._lib import load
+
+            load().adx_em_graph_destroy(self._h)
+            self._h = None
+            self._keep = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 # ---------------------------------------------------------------- batched float64 E-step

@@ -583,6 +583,72 @@ def run_e2e(args, G_dev, P0, Q0, M, N, K, prec, dev):
                     "steps iterations, loglik checks read back, best P/Q copied to the host"}
 
 
+def run_graphs(args):
+    """Adam-EM iterations launched one by one (two kernels each, through the Python wrapper)
+    against the same iterations replayed from a captured CUDA graph (runs of 4, as between
+    the optimiser's checks every 5th iteration, and one run of 20), at the small configs
+    where an iteration takes tens of microseconds. CUDA events around 20 iterations after 3
+    warm-up ones (the events see the gaps the host leaves between launches)."""
+    import torch
+
+    from adamixture_b200 import ops
+    from adamixture_b200.model.em_adam_gpu import EMAdamOptimizer
+    from adamixture_b200.src.simulate import make_cohort
+
+    dev = torch.device("cuda", 0)
+    out = []
+    for name in ("c1", "c2"):
+        cfg = CONFIGS[name]
+        N, M, K = cfg["N"], cfg["M"], cfg["K"]
+        coh = make_cohort(N, M, K, cfg["F"], cfg["alpha"], cfg["miss"], cfg["seed"])
+        Pq = torch.from_numpy(coh.Pq.astype(np.int32)).to(dev)
+        Qq = torch.from_numpy(coh.Qq.astype(np.int32)).to(dev)
+        G = ops.simulate_packed(Pq, Qq, coh.miss_q, coh.keys)
+        del Pq, Qq
+        rng = np.random.default_rng(cfg["seed"])
+        P0 = torch.from_numpy(np.clip(rng.random((M, K)), 1e-5, 1 - 1e-5)).to(dev)
+        Q0 = np.clip(rng.random((N, K)), 1e-5, 1 - 1e-5)
+        Q0 = torch.from_numpy(Q0 / Q0.sum(1, keepdims=True)).to(dev)
+        for prec in ("f64", "f32", "f16"):
+            P, Q = P0.clone(), Q0.clone()
+            P32, Q32 = (P.float(), Q.float()) if prec != "f64" else (None, None)
+            opt = EMAdamOptimizer(P.shape, Q.shape, HP["lr"], HP["beta1"], HP["beta2"], HP["eps"], dev, prec)
+            ws = ops.em_workspace(M, N, K, prec, dev)
+            for _ in range(3):
+                opt.fused_iteration(G, P, Q, P32, Q32, M, ws)
+            stream = torch.cuda.current_stream(dev)
+            row = {"config": name, "N": N, "M": M, "K": K, "precision": prec}
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+            def timed(fn):
+                torch.cuda.synchronize()
+                e0.record(stream)
+                fn()
+                e1.record(stream)
+                torch.cuda.synchronize()
+                return e0.elapsed_time(e1) / 20 * 1000.0   # us per iteration
+
+            def eager():
+                for _ in range(20):
+                    opt.fused_iteration(G, P, Q, P32, Q32, M, ws)
+            row["eager_us"] = timed(eager)
+            for n in (4, 20):
+                g = ops.EmGraph(G, P, Q, P32, Q32, opt.m_P, opt.v_P, opt.m_Q, opt.v_Q, opt.q_bat, M, n, opt.lr,
+                                opt.beta1, opt.beta2, opt.reg_adam, prec, ws)
+                g.launch(opt._t)     # warm-up replay (the first launch uploads the graph)
+                opt._t += n
+
+                def replay():
+                    for _ in range(20 // n):
+                        g.launch(opt._t)
+                        opt._t += n
+                row[f"graph{n}_us"] = timed(replay)
+                g.close()
+            out.append(row)
+            print(json.dumps(row), flush=True)
+    return out
+
+
 def run_sweep_by_k(args):
     """Sweep time of the float32 SIMT form against the FP16 tensor-core form for K = 2..16
     at two shapes (CUDA events, mean of 10 launches after 3 warm-up launches): the
@@ -1075,6 +1141,8 @@ def main():
     ap.add_argument("--kernels-skip-hessian", dest="kernels_skip_hessian", action="store_true")
     ap.add_argument("--sweep-by-k", dest="sweep_by_k", action="store_true",
                     help="float32 vs FP16 tensor-core sweep time for K = 2..16")
+    ap.add_argument("--graphs", action="store_true",
+                    help="eager vs graph-replayed Adam-EM iterations at the small configs")
     args = ap.parse_args()
     if args.warmup < 3:
         print("bench.py: --warmup must be >= 3", file=sys.stderr)
@@ -1109,6 +1177,10 @@ def main():
     if args.sweep_by_k:
         if rank == 0:
             run_sweep_by_k(args)
+        return
+    if args.graphs:
+        if rank == 0:
+            run_graphs(args)
         return
     run_gpu_arm(args, cfg, rank, world, local_rank)
 

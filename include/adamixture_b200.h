@@ -174,6 +174,23 @@ int adx_em_adam_iteration(const uint8_t* G, int64_t M, int64_t N, int K, int pre
                           double beta1, double beta2, double eps, void* workspace,
                           size_t workspace_bytes, void* stream);
 
+/* n_iters (1..4096) adx_em_adam_iteration calls captured once into a CUDA graph (captured on
+ * a private stream; the same kernels and arguments). Iteration i of a replay takes the Adam
+ * step *step_counter + i (step_counter: one device double that the graph owns for its
+ * lifetime); adx_em_graph_launch(graph, t0, stream) sets it to t0, the steps already taken,
+ * and replays, so the replay equals the eager iterations t0+1 .. t0+n_iters bit for bit.
+ * Pointers, shapes and lr are fixed at capture: every buffer must stay allocated at the same
+ * address until adx_em_graph_destroy. Replaces the per-iteration launches of the reference's
+ * loop (adamixture/model/em_adam_gpu.py:330-333) between log-likelihood checks. */
+int adx_em_graph_create(const uint8_t* G, int64_t M, int64_t N, int K, int precision, double* P,
+                        double* Q, float* P32, float* Q32, double* mP, double* vP, double* mQ,
+                        double* vQ, const double* q_bat, int n_iters, double lr, double beta1,
+                        double beta2, double eps, double* step_counter, void* workspace,
+                        size_t workspace_bytes, void** graph);
+int adx_em_graph_launch(void* graph, double t0, void* stream);
+int adx_em_graph_iterations(void* graph, int* n_iters);
+int adx_em_graph_destroy(void* graph);
+
 /* ---------------------------------------------------------------- batched float64 E-step
  * Several Adam-EM problems on one cohort in one sweep launch: n <= 64 problems, each with its
  * own packed genotypes G[p] (the same matrix, or for a cross-validation fold a copy with the

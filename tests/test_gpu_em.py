@@ -423,3 +423,71 @@ def test_optimiser_from_host_matrix_equals_resident(ops, name, request, monkeypa
         out.append((P.cpu().numpy(), Q.cpu().numpy(), [(it, L) for it, L, _ in tr]))
     assert out[0][2] == out[1][2]
     assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][1], out[1][1])
+
+
+@pytest.mark.parametrize("prec", ["f64", "f32", "f16", "bf16"])
+def test_graph_replay_equals_eager_iterations(ops, synth, prec):
+    # fused iterations captured once into a CUDA graph (adx_em_graph_create) and replayed at
+    # steps t0+1..t0+n: P, Q and the Adam moments equal the eager iterations bit for bit
+    from adamixture_b200.model.em_adam_gpu import EMAdamOptimizer
+
+    d = synth
+    M, N = int(d["M"]), int(d["N"])
+    G = dev_t(d["packed"])
+    runs = []
+    for graphed in (False, True):
+        P, Q = dev_t(d["P0"]).clone(), dev_t(d["Q0"]).clone()
+        P32, Q32 = (P.float(), Q.float()) if prec != "f64" else (None, None)
+        opt = EMAdamOptimizer(P.shape, Q.shape, 0.005, 0.80, 0.88, 1e-8, G.device, prec)
+        ws = ops.em_workspace(M, N, Q.shape[1], prec, G.device)
+        opt.fused_iteration(G, P, Q, P32, Q32, M, ws)            # step 1, eager in both runs
+        if graphed:
+            g = ops.EmGraph(G, P, Q, P32, Q32, opt.m_P, opt.v_P, opt.m_Q, opt.v_Q, opt.q_bat, M, 4, opt.lr,
+                            opt.beta1, opt.beta2, opt.reg_adam, prec, ws)
+            g.launch(1)                                            # steps 2..5
+            g.launch(5)                                            # steps 6..9
+            opt._t = 9
+            g.close()
+            with pytest.raises(RuntimeError):
+                g.launch(9)
+        else:
+            for _ in range(8):
+                opt.fused_iteration(G, P, Q, P32, Q32, M, ws)
+        opt.fused_iteration(G, P, Q, P32, Q32, M, ws)            # step 10
+        runs.append([x.cpu().numpy() for x in (P, Q, opt.m_P, opt.v_P, opt.m_Q, opt.v_Q)])
+    for a, b in zip(*runs):
+        assert np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("name,prec", [("demo", "f64"), ("synth", "f64"), ("synth", "f32"), ("synth", "mixed")])
+def test_optimiser_with_graphs_equals_eager(ops, name, prec, request, monkeypatch):
+    # the optimiser replays the iterations between checks from captured graphs; the fit, the
+    # check trace and the stop point equal those of the eager loop
+    from adamixture_b200.model import em_adam_gpu as em
+
+    d = request.getfixturevalue(name)
+    M, N, K = int(d["M"]), int(d["N"]), int(d["K"])
+    G = dev_t(d["packed"])
+    out = []
+    for graphs in (False, True):
+        monkeypatch.setattr(em, "USE_GRAPHS", graphs)
+        tr = []
+        P, Q = em._optimize_parameters_gpu_once(G, dev_t(d["P0"]).clone(), dev_t(d["Q0"]).clone(), 0.005, 0.80,
+                                                0.88, 1e-8, 10000, 5, K, M, N, 0.5, 1e-4, 3, 0.1, G.device, 8192,
+                                                512, precision=prec, trace=tr)
+        out.append((P.cpu().numpy(), Q.cpu().numpy(), [(it, L) for it, L, _ in tr]))
+    assert out[0][2] == out[1][2]
+    assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][1], out[1][1])
+
+
+def test_graph_rejects_bad_arguments(ops, synth):
+    M, N = int(synth["M"]), int(synth["N"])
+    G = dev_t(synth["packed"])
+    P, Q = dev_t(synth["P0"]).clone(), dev_t(synth["Q0"]).clone()
+    z = [torch.zeros_like(x) for x in (P, P, Q, Q)]
+    q = torch.ones(N, dtype=torch.float64, device=G.device)
+    ws = ops.em_workspace(M, N, Q.shape[1], "f64", G.device)
+    with pytest.raises(Exception, match="n_iters"):
+        ops.EmGraph(G, P, Q, None, None, *z, q, M, 0, 0.005, 0.8, 0.88, 1e-8, "f64", ws)
+    with pytest.raises(ValueError, match="workspace"):
+        ops.EmGraph(G, P, Q, None, None, *z, q, M, 3, 0.005, 0.8, 0.88, 1e-8, "f64", ws[:100])
