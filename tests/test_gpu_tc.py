@@ -114,19 +114,28 @@ def test_bounded_wait_gives_up_and_reports(ops):
     assert ops.tc_wait_selftest(True, 2000) == [0, 0, 0]
 
 
-def test_optimiser_raises_on_a_sweep_timeout(ops, synth):
+def test_optimiser_raises_on_a_sweep_timeout(ops, synth, monkeypatch):
     # a sweep that timed out leaves ADX_ERR_TIMEOUT in its workspace's status word; the
-    # optimiser's next check must raise (here the word is set by hand), and the read clears it
+    # optimiser's next check must raise (here the word is set by hand in the optimiser's own
+    # workspace), and the read clears it
     from adamixture_b200.model.em_adam_gpu import optimize_parameters_gpu
 
     M, N, K = int(synth["M"]), int(synth["N"]), int(synth["K"])
     G = dev_t(synth["packed"])
-    ws = ops.Workspace.get(G.device, ops.em_workspace_bytes(M, N, K, "f16"))
-    ws[:4].copy_(torch.tensor([5, 0, 0, 0], dtype=torch.uint8))
+    made = []
+    plain = ops.em_workspace
+
+    def with_timeout_status(*args, **kw):
+        ws = plain(*args, **kw)
+        ws[:4].copy_(torch.tensor([5, 0, 0, 0], dtype=torch.uint8))
+        made.append(ws)
+        return ws
+
+    monkeypatch.setattr(ops, "em_workspace", with_timeout_status)
     with pytest.raises(RuntimeError, match="status 5"):
         optimize_parameters_gpu(G, dev_t(synth["P0"]), dev_t(synth["Q0"]), 0.005, 0.80, 0.88, 1e-8, 10, 5, K,
                                 M, N, 0.5, 1e-4, 3, 0.1, G.device, 8192, 512, precision="f16")
-    assert ops.em_status(ws, M, N, K, "f16") == 0
+    assert len(made) == 1 and ops.em_status(made[0], M, N, K, "f16") == 0
 
 
 @pytest.mark.parametrize("name", ["demo", "synth"])
