@@ -29,6 +29,7 @@ import time
 import torch
 
 from .. import ops
+from .._lib import AdxError
 
 log = logging.getLogger(__name__)
 
@@ -191,8 +192,16 @@ class _IterationGraphs:
         g = self.cache.get(key)
         if g is None:
             q_bat = opt._sample_counts(self.G, self.M)
-            g = ops.EmGraph(self.G, self.P, self.Q, self.P32, self.Q32, opt.m_P, opt.v_P, opt.m_Q, opt.v_Q, q_bat,
-                            self.M, n, opt.lr, opt.beta1, opt.beta2, opt.reg_adam, opt.precision, self.ws)
+            try:
+                g = ops.EmGraph(self.G, self.P, self.Q, self.P32, self.Q32, opt.m_P, opt.v_P, opt.m_Q, opt.v_Q,
+                                q_bat, self.M, n, opt.lr, opt.beta1, opt.beta2, opt.reg_adam, opt.precision,
+                                self.ws)
+            except AdxError as e:
+                # the capture itself failed (nothing ran): the same iterations, launched one by one
+                log.warning(f"    CUDA graph capture unavailable ({e}); launching iterations one by one.")
+                self.enabled = False
+                self.run(n)
+                return
             self.cache[key] = g
         g.launch(opt._t)
         opt._t += n
