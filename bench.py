@@ -23,8 +23,11 @@ reference's default start (randomized SVD + ALS) to the first check within 1e-6 
 of the plain float32 fit's log-likelihood: float32, FP16, and the learned warm start in
 front of FP16. ``e2e`` = the headline iterations through the public Python API starting
 from pinned host buffers (packed G, P, Q) and ending with P/Q back on the host;
-``roofline`` = the headline's E-step sweep kernel alone (algorithmic bytes:
-ceil(M/4)*N + 4K(3M+2N) per launch) against the measured HBM copy bandwidth;
+``roofline`` = the headline's E-step sweep kernel alone: for the float64 sweep, bound by
+the float64 tensor-core pipe, its 8 M N K useful flops per launch against a cuBLAS float64
+GEMM timed in the same run (the HBM figures, algorithmic bytes ceil(M/4)*N + 4K(3M+2N)
+per launch against the measured copy bandwidth, in its ``hbm`` entry); for the other
+sweeps those HBM figures;
 ``cpu_baseline`` = the reference's own CPU Adam-EM step (its Cython kernels compiled from
 source into oracle/_ref) with its every-5th log-likelihood check, on a 25,000-row SNP
 slice of the same cohort, scaled linearly to the full M.
@@ -89,6 +92,37 @@ def peaks_tensor():
         except (ValueError, KeyError):
             pass
     return 1590.0
+
+
+_FP64_PEAK = {}
+
+
+def fp64_gemm_peak(dev):
+    """Float64 tensor-core peak measured on this GPU in this run: a cuBLAS float64 GEMM of
+    8192^3 (2 n^3 flops), best of 5 launches between CUDA events after one warm-up. The
+    driver's measured-peaks file has HBM and BF16 figures only, so the float64 sweep's
+    denominator is measured here the same way (a library GEMM, burst)."""
+    import torch
+
+    if dev in _FP64_PEAK:
+        return _FP64_PEAK[dev]
+    n = 8192
+    a = torch.rand((n, n), dtype=torch.float64, device=dev)
+    b = torch.rand((n, n), dtype=torch.float64, device=dev)
+    c = torch.matmul(a, b)
+    torch.cuda.synchronize(dev)
+    best = float("inf")
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b, out=c)
+        e1.record()
+        torch.cuda.synchronize(dev)
+        best = min(best, e0.elapsed_time(e1))
+    del a, b, c
+    torch.cuda.empty_cache()
+    _FP64_PEAK[dev] = 2.0 * n ** 3 / (best * 1e-3) / 1e12
+    return _FP64_PEAK[dev]
 
 
 def alg_bytes(M, N, K):
@@ -379,7 +413,9 @@ def time_steps(prec, G, P0, Q0, M_loc, N, K, dev, steps, warmup, sharded, clocks
 def sweep_roofline(prec, G, P, Q, M_loc, N, K, dev, reps):
     """The E-step sweep kernel alone (this rank's rows): mean of ``reps`` launches between
     CUDA events on its stream, after one warm-up launch; algorithmic bytes per launch
-    ceil(M/4) N + 4K(3M+2N) against the measured HBM copy bandwidth."""
+    ceil(M/4) N + 4K(3M+2N) against the measured HBM copy bandwidth, and for the float64
+    sweep (bound by the float64 tensor-core pipe) 8 M N K flops against the float64 GEMM
+    peak measured in this run."""
     import torch
 
     from adamixture_b200 import ops
@@ -413,12 +449,18 @@ def sweep_roofline(prec, G, P, Q, M_loc, N, K, dev, reps):
                           "frac": flops / (sweep_ms * 1e-3) / 1e12 / tf if tf else None,
                           "flops_per_launch": flops}
     elif prec == "f64":
-        # the same contractions in float64, against B200's nominal float64 rate (no measured
-        # float64 peak exists for this pool)
-        roof["fp64"] = {"achieved_tflops": flops / (sweep_ms * 1e-3) / 1e12,
-                        "peak_tflops": FP64_NOMINAL_TFLOPS, "peak_kind": "nominal",
-                        "frac": flops / (sweep_ms * 1e-3) / 1e12 / FP64_NOMINAL_TFLOPS,
-                        "flops_per_launch": flops}
+        # The float64 sweep is bound by the float64 tensor-core pipe, not by HBM (8 M N K
+        # flops against 0.25 B per entry): its roofline is the useful contraction flops
+        # against the float64 GEMM peak measured in this run; the HBM figures stay beside it.
+        tflops = flops / (sweep_ms * 1e-3) / 1e12
+        pk = fp64_gemm_peak(G.device)
+        hbm_part = {k: roof[k] for k in ("achieved", "peak", "unit", "frac", "peak_kind")}
+        roof.update({"bound": "tensor", "achieved": tflops, "peak": pk, "unit": "TFLOP/s",
+                     "frac": tflops / pk,
+                     "peak_kind": "measured in this run: cuBLAS float64 GEMM 8192^3, best of 5",
+                     "flops_per_launch": flops, "hbm": hbm_part,
+                     "fp64_nominal": {"peak_tflops": FP64_NOMINAL_TFLOPS,
+                                      "frac": tflops / FP64_NOMINAL_TFLOPS}})
     return roof
 
 
