@@ -56,6 +56,9 @@ SIGNATURES: dict[str, list] = {
     "adx_em_loglik_from_sweep": [P, c_size_t, I64, I64, c_int, c_int, P, P],
     "adx_em_adam_update": [I64, I64, c_int, c_int, P, P, P, P, P, P, P, P, P, c_double, c_double, c_double,
                            c_double, c_double, P, c_size_t, P],
+    "adx_dmma_tiles": [c_int, P],
+    "adx_dmma_tile_set": [c_int, c_int, c_int],
+    "adx_dmma_tile_get": [c_int, c_int, P],
     "adx_loglik_workspace_bytes": [I64, I64, c_int, c_int, P],
     "adx_loglik": [P, I64, I64, c_int, c_int, P, P, P, P, c_size_t, P],
     "adx_loglik_noalloc": [P, I64, I64, c_int, c_int, P, P, P, P],

@@ -31,6 +31,8 @@
 // the MMA accumulators for the whole SNP block and is written once per sub-tile.
 // Shared-memory layouts are chosen so that every fragment load and store is free of bank
 // conflicts (row strides and column swizzles below).
+#include <atomic>
+
 #include "common.cuh"
 
 namespace adx {
@@ -60,6 +62,47 @@ constexpr size_t SMEM_BYTES = sizeof(double) * SMEM_DOUBLES;
 
 __device__ __forceinline__ int qsw(int r) { return ((r >> 3) & 3) << 2; }
 __device__ __forceinline__ int dsw(int r) { return ((r >> 3) & 3) << 2; }
+
+// Shared-memory layouts of the sweep ("tiles"). A layout decides only where the Q and P
+// tiles and the A/B reduction values sit in shared memory, how many SNPs one P group
+// stages, and how many CTAs share an SM -- never the arithmetic or its order, so every
+// layout gives bit-identical statistics and partial sums.
+//   0 (any K <= 16): Q rows of 24 doubles (16 columns, swizzled by Lay<0>::sw = qsw), P groups of 8
+//     chunks in rows of 20, 16 A/B values a thread in the reduction buffers; 174 KiB, one
+//     CTA per SM (up to 255 registers a thread).
+//   1 (K <= 8): Q rows of 16 doubles (8 columns, swizzled by Lay<1>::sw), P groups of 4
+//     chunks in rows of 12, 8 A/B values a thread; 112 KiB and at most 128 registers a
+//     thread, so two CTAs share an SM.
+// Both layouts' fragment loads and stores were checked exhaustively (every half-warp of
+// every access pattern) to be free of bank conflicts.
+template <int TL> struct Lay;
+template <> struct Lay<0> {
+  static constexpr int QSTR = 24, QC = 16, PSTR = 20, PC = 16, GRP = 8, NV = 16, OCC = 1, KSMAX = 4;
+  static __device__ __forceinline__ int sw(int r) { return ((r >> 3) & 3) << 2; }
+};
+template <> struct Lay<1> {
+  static constexpr int QSTR = 16, QC = 8, PSTR = 12, PC = 8, GRP = 4, NV = 8, OCC = 2, KSMAX = 2;
+  static __device__ __forceinline__ int sw(int r) { return (((r >> 3) & 3) << 2) ^ ((r & 1) << 3); }
+};
+// Offsets (doubles) of a layout's regions: Q tile, P group, transpose tiles, A/B reduction
+// buffers (two), per-warp sums.
+template <int TL> struct Off {
+  using L = Lay<TL>;
+  static constexpr int GS = CH * L::GRP;
+  static constexpr int Q = 0;
+  static constexpr int P = Q + W * L::QSTR;
+  static constexpr int D = P + GS * L::PSTR;
+  static constexpr int R = D + WARPS * WS * DSTR;
+  static constexpr int S = R + 2 * WARPS * L::NV * 32;
+  static constexpr int DOUBLES = S + WARPS * WS;
+  static constexpr size_t BYTES = sizeof(double) * DOUBLES;
+  static constexpr int RU = L::NV * 32 / TPB;   // A/B values a thread sums over the warps per chunk
+  static constexpr int NVH = L::NV / 2;         // A values first, then B
+  static_assert(NVH == 4 || NVH == 8, "one or two column tiles");
+};
+static_assert(Off<0>::BYTES == SMEM_BYTES, "layout 0 is the original map");
+static_assert(2 * (Off<1>::BYTES + 1024) <= 228 * 1024, "two layout-1 CTAs fit in an SM's shared memory");
+static_assert(Off<1>::RU * TPB == Lay<1>::NV * 32, "reduction values divide over the threads");
 
 __device__ __forceinline__ void mma_f64(double (&d)[4], double a0, double a1, double b0) {
   asm volatile("mma.sync.aligned.m16n8k4.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5}, {%6}, {%0,%1,%2,%3};"
@@ -178,16 +221,20 @@ struct Probs {
 // block in groups of 8 chunks of 16 SNPs, then the sub-tile's T partials.
 // LL: also multiply every entry's log-likelihood factor into (prod, ex), in the order and
 // arithmetic of loglik_dmma_kernel, so the CTA's partial equals that kernel's.
-template <int KS, bool LL>
+template <int KS, bool LL, int TL>
 __device__ __forceinline__ void sweep_subtile(const Args& a, const Prob& pr, int64_t st, int split, int mblk,
                                               int& chunk_no, double* sm, double& prod, int& ex) {
+  using L = Lay<TL>;
+  using O = Off<TL>;
+  static_assert(KS <= L::KSMAX, "the layout holds the K columns");
   constexpr int NK = (KS + 1) / 2;
-  double* qt = sm + Q_OFF;   // [W][QSTR]: Q rows of the sub-tile, columns swizzled by qsw(row)
-  double* pt = sm + P_OFF;   // [GS][PSTR]: P rows of the group
+  constexpr int QSTR = L::QSTR, PSTR = L::PSTR, GS = O::GS, NV = L::NV, RU = O::RU, NVH = O::NVH;
+  double* qt = sm + O::Q;    // [W][QSTR]: Q rows of the sub-tile, columns swizzled by L::sw(row)
+  double* pt = sm + O::P;    // [GS][PSTR]: P rows of the group
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int g = lane >> 2, t = lane & 3;
-  double* dT = sm + D_OFF + warp * WS * DSTR;  // [WS][DSTR]: d^T of the warp's tile
-  double* sbuf = sm + S_OFF + warp * WS;
+  double* dT = sm + O::D + warp * WS * DSTR;  // [WS][DSTR]: d^T of the warp's tile
+  double* sbuf = sm + O::S + warp * WS;
   const int64_t N = a.N, M = a.M;
   const int64_t j0 = (int64_t)mblk * a.mb;
   const int64_t j1 = min(M, j0 + a.mb);
@@ -198,10 +245,10 @@ __device__ __forceinline__ void sweep_subtile(const Args& a, const Prob& pr, int
     const int64_t i0 = st * W;
     // Q rows of the sub-tile (zero beyond N and K); the previous sub-tile's last reads of
     // qt and pt came before its last chunk barrier
-    for (int e = threadIdx.x; e < W * 16; e += TPB) {
-      const int r = e >> 4, k = e & 15;
+    for (int e = threadIdx.x; e < W * L::QC; e += TPB) {
+      const int r = e / L::QC, k = e % L::QC;
       const int64_t i = i0 + r;
-      qt[r * QSTR + (k ^ qsw(r))] = (i < N && k < K) ? pr.Q[i * K + k] : 0.0;
+      qt[r * QSTR + (k ^ L::sw(r))] = (i < N && k < K) ? pr.Q[i * K + k] : 0.0;
     }
     double tacc[2][NK][4];
     double sb[4][2];
@@ -223,8 +270,8 @@ __device__ __forceinline__ void sweep_subtile(const Args& a, const Prob& pr, int
 
     for (int64_t gj = j0; gj < j1; gj += GS) {
       const int gn = (int)min((int64_t)GS, j1 - gj);
-      for (int e = threadIdx.x; e < GS * 16; e += TPB) {
-        const int r = e >> 4, k = e & 15;
+      for (int e = threadIdx.x; e < GS * L::PC; e += TPB) {
+        const int r = e / L::PC, k = e % L::PC;
         pt[r * PSTR + k] = (r < gn && k < K) ? pr.P[(gj + r) * K + k] : 0.0;
       }
       __syncthreads();
@@ -249,11 +296,11 @@ __device__ __forceinline__ void sweep_subtile(const Args& a, const Prob& pr, int
 #pragma unroll
           for (int u = 0; u < RU; ++u) {
             const int e = threadIdx.x + u * TPB;
-            const int v = e >> 5, l = e & 31, n = (v >> 2) & 1, el = v & 3;
+            const int v = e >> 5, l = e & 31, n = (v >> 2) & (NVH / 4 - 1), el = v & 3;
             const int row = (l >> 2) + 8 * (el >> 1);
             const int col = 8 * n + 2 * (l & 3) + (el & 1);
             if (n < NK && col < K && jc + row < j1)
-              old_ab[u] = pr.ABp[((int64_t)split * M + jc + row) * (2 * K) + (v < 8 ? col : K + col)];
+              old_ab[u] = pr.ABp[((int64_t)split * M + jc + row) * (2 * K) + (v < NVH ? col : K + col)];
           }
         }
         // P fragments: H's A operand (rows g, g+8; columns 4ks + t)
@@ -275,7 +322,7 @@ __device__ __forceinline__ void sweep_subtile(const Args& a, const Prob& pr, int
           const int qrow_h = warp * WS + 8 * (g >> 1) + (g & 1);
 #pragma unroll
           for (int ks = 0; ks < KS; ++ks)
-            if (ks < ksp) mma_f64(hcur, ph[ks][0], ph[ks][1], qt[qrow_h * QSTR + ((4 * ks + t) ^ qsw(qrow_h))]);
+            if (ks < ksp) mma_f64(hcur, ph[ks][0], ph[ks][1], qt[qrow_h * QSTR + ((4 * ks + t) ^ L::sw(qrow_h))]);
         }
 #pragma unroll
         for (int nt = 0; nt < 4; ++nt) {
@@ -285,7 +332,7 @@ __device__ __forceinline__ void sweep_subtile(const Args& a, const Prob& pr, int
             hnext[0] = hnext[1] = hnext[2] = hnext[3] = 0.0;
 #pragma unroll
             for (int ks = 0; ks < KS; ++ks)
-              if (ks < ksp) mma_f64(hnext, ph[ks][0], ph[ks][1], qt[qrow_h * QSTR + ((4 * ks + t) ^ qsw(qrow_h))]);
+              if (ks < ksp) mma_f64(hnext, ph[ks][0], ph[ks][1], qt[qrow_h * QSTR + ((4 * ks + t) ^ L::sw(qrow_h))]);
           }
           const double (&hacc)[4] = hcur;
           if constexpr (LL) ll_factors(hacc, w, nt, prod, ex);
@@ -319,7 +366,7 @@ __device__ __forceinline__ void sweep_subtile(const Args& a, const Prob& pr, int
 #pragma unroll
             for (int n = 0; n < NK; ++n) {
               if (n >= nkp) continue;
-              const double qb = qt[qrow * QSTR + ((8 * n + g) ^ qsw(qrow))];
+              const double qb = qt[qrow * QSTR + ((8 * n + g) ^ L::sw(qrow))];
               mma_f64(aacc[n], av[c], av[2 + c], qb);
               mma_f64(bacc[n], bv[c], bv[2 + c], qb);
             }
@@ -347,22 +394,22 @@ __device__ __forceinline__ void sweep_subtile(const Args& a, const Prob& pr, int
           }
         }
         // A/B of the chunk: this warp's share into the reduction buffer
-        double* red = sm + R_OFF + (chunk_no & 1) * (WARPS * NV * 32);
+        double* red = sm + O::R + (chunk_no & 1) * (WARPS * NV * 32);
 #pragma unroll
         for (int n = 0; n < NK; ++n)
 #pragma unroll
           for (int e = 0; e < 4; ++e) {
             red[(warp * NV + n * 4 + e) * 32 + lane] = aacc[n][e];
-            red[(warp * NV + 8 + n * 4 + e) * 32 + lane] = bacc[n][e];
+            red[(warp * NV + NVH + n * 4 + e) * 32 + lane] = bacc[n][e];
           }
         __syncthreads();
-        // sum over the warps in a fixed order; value v of lane l is (A if v < 8 else B),
-        // column tile (v / 4) % 2, element v % 4 of lane l's fragment
+        // sum over the warps in a fixed order; value v of lane l is (A if v < NV/2 else B),
+        // column tile (v / 4) mod (NV / 8), element v % 4 of lane l's fragment
 #pragma unroll
         for (int u = 0; u < RU; ++u) {
           const int e = threadIdx.x + u * TPB;
           const int v = e >> 5, l = e & 31;
-          const int n = (v >> 2) & 1;
+          const int n = (v >> 2) & (NVH / 4 - 1);
           if (n >= nkp) continue;
           const int el = v & 3;
           const int row = (l >> 2) + 8 * (el >> 1);
@@ -372,7 +419,7 @@ __device__ __forceinline__ void sweep_subtile(const Args& a, const Prob& pr, int
           double s = 0.0;
 #pragma unroll
           for (int ww = 0; ww < WARPS; ++ww) s += red[(ww * NV + v) * 32 + l];
-          double* dst = pr.ABp + ((int64_t)split * M + j) * (2 * K) + (v < 8 ? col : K + col);
+          double* dst = pr.ABp + ((int64_t)split * M + j) * (2 * K) + (v < NVH ? col : K + col);
           *dst = first ? s : old_ab[u] + s;
         }
         ++chunk_no;
@@ -428,8 +475,9 @@ __device__ __forceinline__ void sweep_subtile(const Args& a, const Prob& pr, int
 // other problems.
 // LL (single problem only): the sweep also sums the log-likelihood of its input (P, Q) into
 // a.llp[blockIdx.x], bit-identical to loglik_dmma_kernel's partials.
-template <int KS, int MAXP, bool LL>
-__global__ void __launch_bounds__(TPB, 1) em_sweep_dmma_kernel(Args a, Probs<MAXP> ps) {
+// TL: the shared-memory layout (Lay<TL>); it sets how many CTAs share an SM.
+template <int KS, int MAXP, bool LL, int TL>
+__global__ void __launch_bounds__(TPB, Lay<TL>::OCC) em_sweep_dmma_kernel(Args a, Probs<MAXP> ps) {
   static_assert(!LL || MAXP == 1, "the log-likelihood rides on single-problem sweeps");
   extern __shared__ __align__(16) double sm[];
   const int mblk = a.mblk0 + (int)(blockIdx.x % a.nmb);
@@ -441,18 +489,22 @@ __global__ void __launch_bounds__(TPB, 1) em_sweep_dmma_kernel(Args a, Probs<MAX
     const Prob pr = ps.p[pi];
     for (int64_t st = split; st < a.n_stile; st += a.n_split) {
       if constexpr (MAXP == 1) {
-        sweep_subtile<KS, LL>(a, pr, st, split, mblk, chunk_no, sm, prod, ex);
+        sweep_subtile<KS, LL, TL>(a, pr, st, split, mblk, chunk_no, sm, prod, ex);
+      } else if constexpr (Lay<TL>::KSMAX <= 2) {
+        // the host launches this layout only for batches whose every K is <= 8
+        if (((pr.K + 3) >> 2) == 1) sweep_subtile<1, false, TL>(a, pr, st, split, mblk, chunk_no, sm, prod, ex);
+        else sweep_subtile<2, false, TL>(a, pr, st, split, mblk, chunk_no, sm, prod, ex);
       } else {
         switch ((pr.K + 3) >> 2) {
-          case 1: sweep_subtile<1, false>(a, pr, st, split, mblk, chunk_no, sm, prod, ex); break;
-          case 2: sweep_subtile<2, false>(a, pr, st, split, mblk, chunk_no, sm, prod, ex); break;
-          case 3: sweep_subtile<3, false>(a, pr, st, split, mblk, chunk_no, sm, prod, ex); break;
-          default: sweep_subtile<4, false>(a, pr, st, split, mblk, chunk_no, sm, prod, ex); break;
+          case 1: sweep_subtile<1, false, TL>(a, pr, st, split, mblk, chunk_no, sm, prod, ex); break;
+          case 2: sweep_subtile<2, false, TL>(a, pr, st, split, mblk, chunk_no, sm, prod, ex); break;
+          case 3: sweep_subtile<3, false, TL>(a, pr, st, split, mblk, chunk_no, sm, prod, ex); break;
+          default: sweep_subtile<4, false, TL>(a, pr, st, split, mblk, chunk_no, sm, prod, ex); break;
         }
       }
     }
   }
-  if constexpr (LL) ll_block_sum(prod, ex, sm + S_OFF, a.llp + blockIdx.x);
+  if constexpr (LL) ll_block_sum(prod, ex, sm + Off<TL>::S, a.llp + blockIdx.x);
 }
 
 // ---------------------------------------------------------------- float64 log-likelihood
@@ -547,19 +599,50 @@ __global__ void __launch_bounds__(TPB, 2) loglik_dmma_kernel(Args a, const uint8
 int dmma_plan_width() { return dm::W; }
 int dmma_plan_chunk() { return dm::CH; }
 
-template <int KS, int MAXP, bool LL = false>
+template <int KS, int MAXP, bool LL, int TL>
 static int dmma_launch(const dm::Args& a, const dm::Probs<MAXP>& ps, cudaStream_t st) {
   static bool attr_set[64] = {false};
   int dev = 0;
   ADX_CUDA_TRY(cudaGetDevice(&dev));
   if (dev >= 0 && dev < 64 && !attr_set[dev]) {
-    ADX_CUDA_TRY(cudaFuncSetAttribute(dm::em_sweep_dmma_kernel<KS, MAXP, LL>,
-                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dm::SMEM_BYTES));
+    ADX_CUDA_TRY(cudaFuncSetAttribute(dm::em_sweep_dmma_kernel<KS, MAXP, LL, TL>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dm::Off<TL>::BYTES));
+    // all of the unified L1/shared storage as shared memory, so that OCC CTAs fit on an SM
+    ADX_CUDA_TRY(cudaFuncSetAttribute(dm::em_sweep_dmma_kernel<KS, MAXP, LL, TL>,
+                                      cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared));
     attr_set[dev] = true;
   }
-  dm::em_sweep_dmma_kernel<KS, MAXP, LL><<<(unsigned)(a.n_split * a.nmb), dm::TPB, dm::SMEM_BYTES, st>>>(a, ps);
+  dm::em_sweep_dmma_kernel<KS, MAXP, LL, TL>
+      <<<(unsigned)(a.n_split * a.nmb), dm::TPB, dm::Off<TL>::BYTES, st>>>(a, ps);
   ADX_LAUNCH_CHECK();
   return ADX_OK;
+}
+
+// The layout each (device, K) launches its float64 sweeps with, set by adx_dmma_tile_set
+// (the autotuner's choice) and read at every launch: 0 until set. Layouts never change
+// the results, so a choice made while other threads launch only changes their speed.
+constexpr int DMMA_TILE_DEVICES = 64;
+static std::atomic<int> g_dmma_tile[DMMA_TILE_DEVICES][17];
+
+int dmma_tile_count(int K) { return (K >= 1 && K <= 8) ? 2 : (K >= 9 && K <= 16) ? 1 : 0; }
+
+static int dmma_tile_of(int K) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= DMMA_TILE_DEVICES || K < 1 || K > 16) return 0;
+  const int tl = g_dmma_tile[dev][K].load(std::memory_order_relaxed);
+  return tl < dmma_tile_count(K) ? tl : 0;
+}
+
+int dmma_tile_set(int device, int K, int tile) {
+  if (device < 0 || device >= DMMA_TILE_DEVICES || K < 1 || K > 16 || tile < 0 || tile >= dmma_tile_count(K))
+    return ADX_ERR_ARG;
+  g_dmma_tile[device][K].store(tile, std::memory_order_relaxed);
+  return ADX_OK;
+}
+
+int dmma_tile_get(int device, int K) {
+  if (device < 0 || device >= DMMA_TILE_DEVICES || K < 1 || K > 16) return -1;
+  return g_dmma_tile[device][K].load(std::memory_order_relaxed);
 }
 
 static int dmma_vec(const uint8_t* G, int64_t N) {
@@ -580,18 +663,21 @@ int dmma_sweep(const uint8_t* G, const double* P, const double* Q, int64_t M, in
   dm::Probs<1> ps;
   ps.p[0] = dm::Prob{G, P, Q, ABp, Tp, K, dmma_vec(G, N)};
   ps.n = 1;
-#define ADX_DM_ONE(KS) return llp ? dmma_launch<KS, 1, true>(a, ps, st) : dmma_launch<KS, 1, false>(a, ps, st)
+  const int tl = dmma_tile_of(K);
+#define ADX_DM_ONE(KS, TL) \
+  return llp ? dmma_launch<KS, 1, true, TL>(a, ps, st) : dmma_launch<KS, 1, false, TL>(a, ps, st)
   switch ((K + 3) / 4) {
-    case 1: ADX_DM_ONE(1);
-    case 2: ADX_DM_ONE(2);
-    case 3: ADX_DM_ONE(3);
-    default: ADX_DM_ONE(4);
+    case 1: if (tl == 1) { ADX_DM_ONE(1, 1); } ADX_DM_ONE(1, 0);
+    case 2: if (tl == 1) { ADX_DM_ONE(2, 1); } ADX_DM_ONE(2, 0);
+    case 3: ADX_DM_ONE(3, 0);
+    default: ADX_DM_ONE(4, 0);
   }
 #undef ADX_DM_ONE
 }
 
 constexpr int DMMA_MAX_PROBLEMS = 64;
 
+// A batch launches with layout 1 when every problem's K has layout 1 selected, else 0.
 int dmma_sweep_batch(int64_t M, int64_t N, int n, const int* K, const uint8_t* const* G, const double* const* P,
                      const double* const* Q, double* const* ABp, double* const* Tp, int64_t n_stile, int n_split,
                      int n_mblk, int64_t mb, cudaStream_t st) {
@@ -599,12 +685,15 @@ int dmma_sweep_batch(int64_t M, int64_t N, int n, const int* K, const uint8_t* c
   dm::Args a{M, N, n_stile, n_split, n_mblk, mb, nullptr};
   a.nmb = n_mblk;
   dm::Probs<DMMA_MAX_PROBLEMS> ps;
+  bool all1 = true;
   for (int p = 0; p < n; ++p) {
     if (K[p] < 1 || K[p] > 16 || !G[p]) return ADX_ERR_ARG;
     ps.p[p] = dm::Prob{G[p], P[p], Q[p], ABp[p], Tp[p], K[p], dmma_vec(G[p], N)};
+    all1 = all1 && dmma_tile_of(K[p]) == 1;
   }
   ps.n = n;
-  return dmma_launch<4, DMMA_MAX_PROBLEMS>(a, ps, st);
+  return all1 ? dmma_launch<2, DMMA_MAX_PROBLEMS, false, 1>(a, ps, st)
+              : dmma_launch<4, DMMA_MAX_PROBLEMS, false, 0>(a, ps, st);
 }
 
 }  // namespace adx
@@ -651,3 +740,24 @@ int dmma_loglik(const uint8_t* G, const double* P, const double* Q, int64_t M, i
 }
 
 }  // namespace adx
+
+// ---------------------------------------------------------------- tile choice (C ABI)
+
+extern "C" int adx_dmma_tiles(int K, int* count) {
+  if (!count || K < 1 || K > 16) { adx_set_message("adx_dmma_tiles: K must be in 1..16"); return ADX_ERR_ARG; }
+  *count = adx::dmma_tile_count(K);
+  return ADX_OK;
+}
+
+extern "C" int adx_dmma_tile_set(int device, int K, int tile) {
+  const int rc = adx::dmma_tile_set(device, K, tile);
+  if (rc) adx_set_message("adx_dmma_tile_set: device, K (1..16) or tile (< adx_dmma_tiles) out of range");
+  return rc;
+}
+
+extern "C" int adx_dmma_tile_get(int device, int K, int* tile) {
+  const int tl = tile ? adx::dmma_tile_get(device, K) : -1;
+  if (tl < 0) { adx_set_message("adx_dmma_tile_get: device or K (1..16) out of range"); return ADX_ERR_ARG; }
+  *tile = tl;
+  return ADX_OK;
+}

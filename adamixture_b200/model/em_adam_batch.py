@@ -4,8 +4,9 @@ The reference runs the K sweep one K at a time (adamixture/src/main.py:67-107) a
 cross-validation per K and fold afterwards (adamixture/src/cv.py:171-267). Here a list of
 problems -- each with its own K (<= 16), start, Adam state and learning-rate schedule, and
 optionally a cross-validation fold whose entries it treats as missing -- advances together:
-every iteration is ONE launch of the batched float64 E-step sweep, then each problem's EM
-targets and Adam move. Each CTA of the sweep runs the problems in order over its share of
+every iteration is one launch of the batched float64 E-step sweep per tile layout in use
+(one launch, or two when the autotuner runs the K <= 8 problems on the two-CTA-per-SM
+layout and the others on the default one), then each problem's EM targets and Adam move. Each CTA of the sweep runs the problems in order over its share of
 the matrix, so problems on the same genotypes (all full-data fits; all problems of one
 fold) read them from memory once and from L2 after that.
 
@@ -28,7 +29,7 @@ from dataclasses import dataclass, field
 
 import torch
 
-from .. import ops
+from .. import ops, tune
 from .em_adam_gpu import EMAdamOptimizer, optimize_parameters_gpu
 
 log = logging.getLogger(__name__)
@@ -89,14 +90,27 @@ def _prepare(G, M, problems, seed, n_buckets):
 
 
 def _iteration(M, N, live):
-    """One batched sweep over the live problems, then each one's targets + Adam move."""
-    batch = ops.EmBatch(M, N, [p.K for p in live], live[0].G.device)
-    batch.sweep([p.G for p in live], [p.P for p in live], [p.Q for p in live])
-    for k, pr in enumerate(live):
-        pr.t += 1.0
-        batch.adam(k, pr.P, pr.Q, pr.mP, pr.vP, pr.mQ, pr.vQ, pr.q_bat, pr.t, pr.lr, HP["beta1"], HP["beta2"],
-                   HP["eps"])
-        pr.iterations += 1
+    """One batched sweep over the live problems, then each one's targets + Adam move. A
+    batched sweep launches one tile layout, so problems whose K runs another layout (the
+    autotuner's choice, ``tune.batch_groups``) go in a launch of their own."""
+    for idx in tune.batch_groups([p.K for p in live], live[0].G.device):
+        group = [live[i] for i in idx]
+        batch = ops.EmBatch(M, N, [p.K for p in group], group[0].G.device)
+        batch.sweep([p.G for p in group], [p.P for p in group], [p.Q for p in group])
+        for k, pr in enumerate(group):
+            pr.t += 1.0
+            batch.adam(k, pr.P, pr.Q, pr.mP, pr.vP, pr.mQ, pr.vQ, pr.q_bat, pr.t, pr.lr, HP["beta1"],
+                       HP["beta2"], HP["eps"])
+            pr.iterations += 1
+
+
+def _tune(G, M, problems):
+    """The float64 sweep's layout for every K of the batch (once per shape and K)."""
+    seen = set()
+    for pr in problems:
+        if pr.K not in seen and pr.K <= 16:
+            seen.add(pr.K)
+            tune.tune_dmma(pr.G, pr.P, pr.Q, M)
 
 
 def optimize_batch(G, M, N, problems, seed=0, n_buckets=10, max_iter=10000, check=5, lr_decay=0.5,
@@ -112,6 +126,7 @@ def optimize_batch(G, M, N, problems, seed=0, n_buckets=10, max_iter=10000, chec
     Returns the problems (results in ``P_best``/``Q_best``)."""
     problems = sorted(problems, key=lambda p: p.fold)   # problems on the same genotypes adjacent
     _prepare(G, M, problems, seed, n_buckets)
+    _tune(G, M, problems)
     if fixed_iters is not None:
         for _ in range(int(fixed_iters)):
             _iteration(M, N, problems)

@@ -28,7 +28,7 @@ import time
 
 import torch
 
-from .. import ops
+from .. import ops, tune
 from .._lib import AdxError
 
 log = logging.getLogger(__name__)
@@ -253,6 +253,8 @@ def _optimize_parameters_gpu_once(G, P, Q, lr, beta1, beta2, reg_adam, max_iter,
     P32 = P.to(torch.float32).contiguous() if dt == torch.float32 else None
     Q32 = Q.to(torch.float32).contiguous() if dt == torch.float32 else None
     ws = ops.em_workspace(M, N, K, prec, G.device)
+    if prec == "f64" and K <= 16:
+        tune.tune_dmma(G, P, Q, M, workspace=ws)
 
     def loglik():
         if ll_prec == "f64":
@@ -495,6 +497,9 @@ def _optimize_streamed(G_host, P, Q, lr, beta1, beta2, reg_adam, max_iter, check
     t_start = time.perf_counter()
     G, ws = _upload_and_prime(G_host, P, Q, M, K, opt, device)
     log.info(f"    Performed priming iteration... ({time.time() - ts:.1f}s)\n")
+    # the priming sweep ran the default layout; the loop's sweeps run the tuned one (the
+    # tuning sweeps overwrite only partial sums that the loop's first sweep rewrites)
+    tune.tune_dmma(G, P, Q, M, workspace=ws)
     return _loop_folded_checks(G, P, Q, M, N, K, opt, ws, max_iter, check, lr_decay, min_lr, patience, tol_adam,
                                trace, t_start)
 

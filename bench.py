@@ -732,6 +732,58 @@ def run_sweep_by_k(args):
     print(json.dumps({"metric": "E-step sweep ms by K", "rows": out}), flush=True)
 
 
+def run_tiles(args):
+    """``--tiles``: the float64 sweep under each of its tile layouts for K = 2..12 at the
+    config-4 shape (N=20,000 x M=100,000) and at K=3 / 8 / 10 at the c1, c2 and c3 shapes
+    (CUDA events, mean of 5 launches after one warm-up), with the autotuner's pick for
+    each (its own timing, a partial sweep over whole waves). The layouts give
+    bit-identical partial sums; the line says so per row."""
+    import torch
+
+    from adamixture_b200 import ops, tune
+    from adamixture_b200.src.simulate import make_cohort
+
+    dev = torch.device("cuda", 0)
+    cases = [(20_000, 100_000, K) for K in range(2, 13)] + [(1_000, 10_000, 3), (10_000, 200_000, 8),
+                                                          (200_000, 500_000, 8), (200_000, 500_000, 10)]
+    rows, cache = [], {}
+    for N, M, K in cases:
+        if (N, M) not in cache:
+            cache.clear()
+            torch.cuda.empty_cache()
+            coh = make_cohort(N, M, 6, 0.05, 0.3, 0.01, 21)
+            cache[(N, M)] = ops.simulate_packed(torch.from_numpy(coh.Pq.astype(np.int32)).to(dev),
+                                                torch.from_numpy(coh.Qq.astype(np.int32)).to(dev),
+                                                coh.miss_q, coh.keys)
+        G = cache[(N, M)]
+        rng = np.random.default_rng(K)
+        P = torch.from_numpy(np.clip(rng.random((M, K)), 1e-5, 1 - 1e-5)).to(dev)
+        Qn = np.clip(rng.random((N, K)), 1e-5, 1 - 1e-5)
+        Q = torch.from_numpy(Qn / Qn.sum(1, keepdims=True)).to(dev)
+        ws = ops.em_workspace(M, N, K, "f64", dev)
+        row = {"N": N, "M": M, "K": K}
+        parts = []
+        for tile in range(tune.tiles(K)):
+            tune.set_tile(K, tile, 0)
+            ops.em_sweep(G, P, Q, M, "f64", ws)
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            for _ in range(5):
+                ops.em_sweep(G, P, Q, M, "f64", ws)
+            e1.record()
+            torch.cuda.synchronize()
+            row[f"layout{tile}_ms"] = e0.elapsed_time(e1) / 5
+            parts.append(ws.clone())
+        row["bit_identical"] = all(torch.equal(parts[0], x) for x in parts[1:])
+        tune.set_tile(K, 0, 0)
+        row["tuned"] = tune.tune_dmma(G, P, Q, M, workspace=ws, force=True)
+        rows.append(row)
+        del ws, parts, P, Q
+        torch.cuda.synchronize()
+    print(json.dumps({"metric": "float64 E-step sweep ms by tile layout", "rows": rows}), flush=True)
+
+
 def run_kernels(args, cfg):
     """Per-kernel timings at the config's shape (CUDA events, mean of ``reps`` launches after
     one warm-up): the randomized-SVD products, the log-likelihood, BVLS, the BR-QN
@@ -1181,6 +1233,8 @@ def main():
     ap.add_argument("--batch-sweeps", dest="batch_sweeps", action="store_true",
                     help="c4: time single and batched sweep launches instead of the CV runs")
     ap.add_argument("--kernels-skip-hessian", dest="kernels_skip_hessian", action="store_true")
+    ap.add_argument("--tiles", action="store_true",
+                    help="float64 sweep time per tile layout and the autotuner's pick, K = 2..12 and c1-c3")
     ap.add_argument("--sweep-by-k", dest="sweep_by_k", action="store_true",
                     help="float32 vs FP16 tensor-core sweep time for K = 2..16")
     ap.add_argument("--graphs", action="store_true",
@@ -1215,6 +1269,9 @@ def main():
     if args.config == "c5":
         if rank == 0:
             run_warm_start(args, cfg)
+        return
+    if args.tiles:
+        run_tiles(args)
         return
     if args.sweep_by_k:
         if rank == 0:

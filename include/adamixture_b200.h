@@ -214,6 +214,20 @@ int adx_em_batch_apply(int64_t M, int64_t N, int n, const int* K, int p, int mod
                        double* mQ, double* vQ, double t, double lr, double beta1, double beta2, double eps,
                        void* workspace, size_t workspace_bytes, void* stream);
 
+/* Shared-memory layouts ("tiles") of the float64 tensor-core sweep, chosen per device and K
+ * by the autotuner (adamixture_b200/tune.py). No counterpart in the reference, whose E-step
+ * has no tile choice (torch matmuls, adamixture/model/em_adam_gpu.py:46-78). A layout only
+ * moves values in shared memory and sets how many CTAs share an SM, so every layout gives
+ * bit-identical results; layout 0 (any K <= 16) is the default until one is set, layout 1
+ * (K <= 8) puts two CTAs on an SM. The choice applies to adx_em_stats, adx_em_sweep,
+ * adx_em_sweep_blocks, adx_em_sweep_loglik and adx_em_adam_iteration at ADX_F64 with
+ * K <= 16, and to a batched sweep (adx_em_sweep_batch) when every problem's K has layout 1
+ * selected. adx_dmma_tiles: the number of layouts for K; adx_dmma_tile_set / _get: the
+ * layout of (device, K). */
+int adx_dmma_tiles(int K, int* count);
+int adx_dmma_tile_set(int device, int K, int tile);
+int adx_dmma_tile_get(int device, int K, int* tile);
+
 /* Binomial log-likelihood, float64 sum: sum over observed entries of
  * g log h + (2-g) log(1-h), h = clamp(P Q^T, 1e-10, 1-1e-10) (loglikelihood_gpu,
  * em_adam_gpu.py:226-279). *out is a device double. */
