@@ -49,7 +49,6 @@ constexpr int QSTR = 24;               // Q tile row stride (doubles); column sw
 constexpr int PSTR = 20;               // P tile row stride (doubles)
 constexpr int DSTR = 20;               // transpose tile row stride (doubles); swizzle dsw()
 constexpr int NV = 16;                 // A/B accumulator values per thread (2 x 2 tiles x 4)
-constexpr int RU = NV * 32 / TPB;      // A/B values a thread sums over the warps per chunk
 
 // shared memory (doubles)
 constexpr int Q_OFF = 0;

@@ -735,17 +735,23 @@ def run_sweep_by_k(args):
 def run_tiles(args):
     """``--tiles``: the float64 sweep under each of its tile layouts for K = 2..12 at the
     config-4 shape (N=20,000 x M=100,000) and at K=3 / 8 / 10 at the c1, c2 and c3 shapes
-    (CUDA events, mean of 5 launches after one warm-up), with the autotuner's pick for
-    each (its own timing, a partial sweep over whole waves). The layouts give
-    bit-identical partial sums; the line says so per row."""
+    (``--config c3s``: K=8 at N=200,000 x M=50,000 only, the profiled case); CUDA events,
+    mean of min(5, --steps) launches after one warm-up, with the autotuner's pick for each
+    (its own timing, a partial sweep over whole waves). The layouts give bit-identical
+    partial sums; the line says so per row."""
     import torch
 
     from adamixture_b200 import ops, tune
     from adamixture_b200.src.simulate import make_cohort
 
     dev = torch.device("cuda", 0)
-    cases = [(20_000, 100_000, K) for K in range(2, 13)] + [(1_000, 10_000, 3), (10_000, 200_000, 8),
-                                                          (200_000, 500_000, 8), (200_000, 500_000, 10)]
+    if args.config == "c3s":
+        # the profiled case: the c3 generator at one tenth of its SNPs (2.5 GB packed), K=8
+        cases = [(200_000, 50_000, 8)]
+    else:
+        cases = [(20_000, 100_000, K) for K in range(2, 13)] + [(1_000, 10_000, 3), (10_000, 200_000, 8),
+                                                              (200_000, 500_000, 8), (200_000, 500_000, 10)]
+    reps = max(1, min(5, args.steps))
     rows, cache = [], {}
     for N, M, K in cases:
         if (N, M) not in cache:
@@ -769,11 +775,11 @@ def run_tiles(args):
             torch.cuda.synchronize()
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record()
-            for _ in range(5):
+            for _ in range(reps):
                 ops.em_sweep(G, P, Q, M, "f64", ws)
             e1.record()
             torch.cuda.synchronize()
-            row[f"layout{tile}_ms"] = e0.elapsed_time(e1) / 5
+            row[f"layout{tile}_ms"] = e0.elapsed_time(e1) / reps
             parts.append(ws.clone())
         row["bit_identical"] = all(torch.equal(parts[0], x) for x in parts[1:])
         tune.set_tile(K, 0, 0)
