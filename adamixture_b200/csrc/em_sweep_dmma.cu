@@ -7,8 +7,8 @@
 // (AB_part[split][j][2K], T_part[snp_block][i][K], float64), so em_update_kernel<double>
 // reduces them unchanged. The CUDA-core form spends most of its issue slots folding the 2K
 // A/B values of every SNP over the warp with shuffles; here the three contractions and h
-// are float64 MMAs (mma.sync m16n8k4 .f64, 512 FMAs per warp instruction) and the CUDA
-// cores do only the per-entry ratios.
+// are float64 MMAs (mma.sync .f64: m16n8k4 for h, m16n8k8 -- 1024 FMAs a warp instruction
+// -- for A, B and T) and the CUDA cores do only the per-entry ratios.
 //
 // CTA: 8 warps over a 256-sample sub-tile, 32 samples per warp, walking the block's SNPs in
 // chunks of 16 (groups of 8 chunks staged in shared memory). (Two 4-warp CTAs per SM ran
@@ -17,15 +17,17 @@
 // x 32-sample tile as four 16 x 8 MMA tiles (fragment element: SNP row g or g+8, columns
 // 2t, 2t+1; g = lane / 4, t = lane % 4). Column j of tile nt is local sample
 // 8 (j / 2) + 2 nt + (j % 2), so a thread's 8 entries per SNP row are 8 consecutive
-// samples (one 8-byte genotype load) and a pair of columns (2t, 2t+1) is a 4-sample chunk
-// of the contraction over samples:
+// samples (one 8-byte genotype load) and the 8 columns of a tile are one 8-sample k-step
+// of the contraction over samples (k-slot t: column 2t, k-slot t + 4: column 2t + 1):
 //   * H (16 x 8 per tile) = P_chunk (16 x K) . Q^T: ceil(K/4) k-steps of 4;
 //   * the ratios a, b per entry; a and b, read straight from the H fragments, are the A
-//     operands of A += a Q and B += b Q (16 SNPs x 8 K-columns per MMA, 4 samples per
-//     k-step; Q as the B operand);
+//     operands of A += a Q and B += b Q (16 SNPs x 8 K-columns per MMA, the tile's 8
+//     samples per k-step; Q as the B operand);
 //   * d = a - b goes through a per-warp shared-memory transpose (samples x SNPs) to become
-//     the A operand of T += d^T P (16 samples x 8 K-columns, 4 SNPs per k-step); sum_j b
+//     the A operand of T += d^T P (16 samples x 8 K-columns, 8 SNPs per k-step); sum_j b
 //     is added per thread and folded over the SNP lanes at the end.
+// An m16n8k8 MMA gives the same float64 results, bit for bit, as the two m16n8k4 MMAs over
+// the same k-slots that it replaced (measured), with half the MMA instructions.
 // A and B of a chunk are summed over the CTA's warps in shared memory (fixed order, double
 // buffered: one barrier per chunk) and added into the block's own AB_part rows; T lives in
 // the MMA accumulators for the whole SNP block and is written once per sub-tile.
@@ -103,6 +105,12 @@ static_assert(Off<0>::BYTES == SMEM_BYTES, "layout 0 is the original map");
 static_assert(2 * (Off<1>::BYTES + 1024) <= 228 * 1024, "two layout-1 CTAs fit in an SM's shared memory");
 static_assert(Off<1>::RU * TPB == Lay<1>::NV * 32, "reduction values divide over the threads");
 
+__device__ __forceinline__ void mma_f64_k8(double (&d)[4], double a0, double a1, double a2, double a3, double b0,
+                                           double b1) {
+  asm volatile("mma.sync.aligned.m16n8k8.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};"
+               : "+d"(d[0]), "+d"(d[1]), "+d"(d[2]), "+d"(d[3])
+               : "d"(a0), "d"(a1), "d"(a2), "d"(a3), "d"(b0), "d"(b1));
+}
 __device__ __forceinline__ void mma_f64(double (&d)[4], double a0, double a1, double b0) {
   asm volatile("mma.sync.aligned.m16n8k4.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5}, {%6}, {%0,%1,%2,%3};"
                : "+d"(d[0]), "+d"(d[1]), "+d"(d[2]), "+d"(d[3])
@@ -358,16 +366,17 @@ __device__ __forceinline__ void sweep_subtile(const Args& a, const Prob& pr, int
           }
           sb[nt][0] += bv[0] + bv[2];
           sb[nt][1] += bv[1] + bv[3];
-          // A += a Q, B += b Q: k-step c of this tile is columns (2t + c): samples 8t + 2nt + c
-#pragma unroll
-          for (int c = 0; c < 2; ++c) {
-            const int qrow = warp * WS + 8 * t + 2 * nt + c;
+          // A += a Q, B += b Q, one 8-sample k-step: k-slot t is column 2t (sample 8t + 2nt),
+          // k-slot t + 4 column 2t + 1 (sample 8t + 2nt + 1)
+          {
+            const int qrow0 = warp * WS + 8 * t + 2 * nt, qrow1 = qrow0 + 1;
 #pragma unroll
             for (int n = 0; n < NK; ++n) {
               if (n >= nkp) continue;
-              const double qb = qt[qrow * QSTR + ((8 * n + g) ^ L::sw(qrow))];
-              mma_f64(aacc[n], av[c], av[2 + c], qb);
-              mma_f64(bacc[n], bv[c], bv[2 + c], qb);
+              const double qb0 = qt[qrow0 * QSTR + ((8 * n + g) ^ L::sw(qrow0))];
+              const double qb1 = qt[qrow1 * QSTR + ((8 * n + g) ^ L::sw(qrow1))];
+              mma_f64_k8(aacc[n], av[0], av[2], av[1], av[3], qb0, qb1);
+              mma_f64_k8(bacc[n], bv[0], bv[2], bv[1], bv[3], qb0, qb1);
             }
           }
           if (nt < 3) {
@@ -376,20 +385,26 @@ __device__ __forceinline__ void sweep_subtile(const Args& a, const Prob& pr, int
           }
         }
         __syncwarp();
-        // T += d^T P: rows = local samples 16 m + g (+8), k-step q = SNPs 4q + t
+        // T += d^T P: rows = local samples 16 m + g (+8), k-step q = SNPs 8q + t (k-slot t) and
+        // 8q + t + 4 (k-slot t + 4)
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
-          double pb[NK];
+        for (int q = 0; q < 2; ++q) {
+          double pb0[NK], pb1[NK];
 #pragma unroll
-          for (int n = 0; n < NK; ++n) pb[n] = pc[(4 * q + t) * PSTR + 8 * n + g];
+          for (int n = 0; n < NK; ++n) {
+            pb0[n] = pc[(8 * q + t) * PSTR + 8 * n + g];
+            pb1[n] = pc[(8 * q + t + 4) * PSTR + 8 * n + g];
+          }
 #pragma unroll
           for (int m = 0; m < 2; ++m) {
             const int r0 = 16 * m + g, r1 = r0 + 8;
-            const double d0 = dT[r0 * DSTR + ((4 * q + t) ^ dsw(r0))];
-            const double d1 = dT[r1 * DSTR + ((4 * q + t) ^ dsw(r1))];
+            const double d0 = dT[r0 * DSTR + ((8 * q + t) ^ dsw(r0))];
+            const double d1 = dT[r1 * DSTR + ((8 * q + t) ^ dsw(r1))];
+            const double d2 = dT[r0 * DSTR + ((8 * q + t + 4) ^ dsw(r0))];
+            const double d3 = dT[r1 * DSTR + ((8 * q + t + 4) ^ dsw(r1))];
 #pragma unroll
             for (int n = 0; n < NK; ++n)
-              if (n < nkp) mma_f64(tacc[m][n], d0, d1, pb[n]);
+              if (n < nkp) mma_f64_k8(tacc[m][n], d0, d1, d2, d3, pb0[n], pb1[n]);
           }
         }
         // A/B of the chunk: this warp's share into the reduction buffer

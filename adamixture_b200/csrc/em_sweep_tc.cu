@@ -207,6 +207,20 @@ __device__ __forceinline__ float rcp_approx(float x) {
   asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
   return r;
 }
+// Packed float32 pairs: mul.rn.f32x2 multiplies both lanes as two scalar IEEE multiplies do.
+__device__ __forceinline__ uint64_t mul_f32x2(uint64_t a, uint64_t b) {
+  uint64_t d;
+  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
+__device__ __forceinline__ uint64_t pack_f32x2(float lo, float hi) {
+  uint64_t r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+  return r;
+}
+__device__ __forceinline__ void unpack_f32x2(uint64_t v, float& lo, float& hi) {
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+}
 __device__ __forceinline__ uint32_t prmt(uint32_t a, uint32_t b, uint32_t sel) {
   uint32_t r;
   asm("prmt.b32 %0, %1, %2, %3;" : "=r"(r) : "r"(a), "r"(b), "r"(sel));
@@ -582,9 +596,16 @@ __global__ void __launch_bounds__(TPB, 1) em_sweep_tc_kernel(Args a) {
             const float rec1 = fmaxf(__uint_as_float(hv[cur][e + 1]), ELO);
             const float omr0 = fmaxf(__uint_as_float(cv[cur][e]), ELO);
             const float omr1 = fmaxf(__uint_as_float(cv[cur][e + 1]), ELO);
-            const float r0 = rcp_approx(rec0 * omr0), r1 = rcp_approx(rec1 * omr1);
-            const uint32_t ypair = F::pack(omr0 * r0, omr1 * r1);  // 1/rec (FP16: 1/(64 rec))
-            const uint32_t xpair = F::pack(rec0 * r0, rec1 * r1);  // 1/(1-rec)
+            // the pair's products as packed float32 multiplies (each lane the scalar product)
+            const uint64_t rr = pack_f32x2(rec0, rec1), oo = pack_f32x2(omr0, omr1);
+            float x0, x1;
+            unpack_f32x2(mul_f32x2(rr, oo), x0, x1);
+            const uint64_t rp = pack_f32x2(rcp_approx(x0), rcp_approx(x1));
+            float y0, y1, z0, z1;
+            unpack_f32x2(mul_f32x2(oo, rp), y0, y1);
+            unpack_f32x2(mul_f32x2(rr, rp), z0, z1);
+            const uint32_t ypair = F::pack(y0, y1);  // 1/rec (FP16: 1/(64 rec))
+            const uint32_t xpair = F::pack(z0, z1);  // 1/(1-rec)
             ap[e >> 1] = F::mul(prmt(F::GA_LO, F::GA_HI, sel), ypair);
             bp[e >> 1] = F::mul(prmt(F::GB_LO, F::GB_HI, sel), xpair);
           }
