@@ -323,23 +323,26 @@ __device__ __forceinline__ void sweep_subtile(const Args& a, const Prob& pr, int
 #pragma unroll
           for (int e = 0; e < 4; ++e) aacc[n][e] = bacc[n][e] = 0.0;
 
-        // H of tile nt + 1 is issued before tile nt's ratios, so the MMAs' latency overlaps them
-        double hcur[4] = {0.0, 0.0, 0.0, 0.0}, hnext[4];
-        {
-          const int qrow_h = warp * WS + 8 * (g >> 1) + (g & 1);
+        // H of tile nt + 1 is issued before tile nt's ratios, so the MMAs' latency overlaps them.
+        // k-steps 2s and 2s+1 of 4 run as one m16n8k8 (k-slots t and t + 4), an odd last one
+        // as an m16n8k4: the same sums as KS k-steps of 4.
+        auto h_tile = [&](double (&hacc)[4], int qrow_h) {
 #pragma unroll
-          for (int ks = 0; ks < KS; ++ks)
-            if (ks < ksp) mma_f64(hcur, ph[ks][0], ph[ks][1], qt[qrow_h * QSTR + ((4 * ks + t) ^ L::sw(qrow_h))]);
-        }
+          for (int ks = 0; ks + 1 < KS; ks += 2)
+            mma_f64_k8(hacc, ph[ks][0], ph[ks][1], ph[ks + 1][0], ph[ks + 1][1],
+                       qt[qrow_h * QSTR + ((4 * ks + t) ^ L::sw(qrow_h))],
+                       qt[qrow_h * QSTR + ((4 * ks + 4 + t) ^ L::sw(qrow_h))]);
+          if constexpr (KS & 1)
+            mma_f64(hacc, ph[KS - 1][0], ph[KS - 1][1], qt[qrow_h * QSTR + ((4 * (KS - 1) + t) ^ L::sw(qrow_h))]);
+        };
+        double hcur[4] = {0.0, 0.0, 0.0, 0.0}, hnext[4];
+        h_tile(hcur, warp * WS + 8 * (g >> 1) + (g & 1));
 #pragma unroll
         for (int nt = 0; nt < 4; ++nt) {
           if (nt < 3) {
             // H tile nt+1: column g of the B operand is local sample 8 (g / 2) + 2 (nt+1) + g % 2
-            const int qrow_h = warp * WS + 8 * (g >> 1) + 2 * (nt + 1) + (g & 1);
             hnext[0] = hnext[1] = hnext[2] = hnext[3] = 0.0;
-#pragma unroll
-            for (int ks = 0; ks < KS; ++ks)
-              if (ks < ksp) mma_f64(hnext, ph[ks][0], ph[ks][1], qt[qrow_h * QSTR + ((4 * ks + t) ^ L::sw(qrow_h))]);
+            h_tile(hnext, warp * WS + 8 * (g >> 1) + 2 * (nt + 1) + (g & 1));
           }
           const double (&hacc)[4] = hcur;
           if constexpr (LL) ll_factors(hacc, w, nt, prod, ex);
@@ -596,9 +599,13 @@ __global__ void __launch_bounds__(TPB, 2) loglik_dmma_kernel(Args a, const uint8
         for (int nt = 0; nt < 4; ++nt) {
           const int qrow = warp * WS + 8 * (g >> 1) + 2 * nt + (g & 1);
           hacc[nt][0] = hacc[nt][1] = hacc[nt][2] = hacc[nt][3] = 0.0;
+          // as in the sweep: k-step pairs on one m16n8k8, an odd last k-step on an m16n8k4
 #pragma unroll
-          for (int ks = 0; ks < KS; ++ks)
-            mma_f64(hacc[nt], ph[ks][0], ph[ks][1], qt[qrow * QSTR + ((4 * ks + t) ^ qsw(qrow))]);
+          for (int ks = 0; ks + 1 < KS; ks += 2)
+            mma_f64_k8(hacc[nt], ph[ks][0], ph[ks][1], ph[ks + 1][0], ph[ks + 1][1],
+                       qt[qrow * QSTR + ((4 * ks + t) ^ qsw(qrow))], qt[qrow * QSTR + ((4 * ks + 4 + t) ^ qsw(qrow))]);
+          if constexpr (KS & 1)
+            mma_f64(hacc[nt], ph[KS - 1][0], ph[KS - 1][1], qt[qrow * QSTR + ((4 * (KS - 1) + t) ^ qsw(qrow))]);
         }
 #pragma unroll
         for (int nt = 0; nt < 4; ++nt) ll_factors(hacc[nt], w, nt, prod, ex);
