@@ -175,14 +175,18 @@ em_sweep_kernel(const uint8_t* __restrict__ G, const R* __restrict__ P, const R*
         for (int s = 0; s < 4; ++s) {
           const int jl = qd + s;
           if (jl >= cn) break;  // uniform across the block
-          R a[SPT], b[SPT];
+          R a[SPT], b[SPT], hh[SPT];
 #pragma unroll
           for (int u = 0; u < SPT; ++u) {
-            const unsigned g = genotype(bytes[u], s);
             R h = 0;
 #pragma unroll
             for (int k = 0; k < KMAX; ++k) h += Ps[jl][k] * q[u][k];
-            const R rec = clampr(h, ELO, EHI);
+            hh[u] = h;
+          }
+#pragma unroll
+          for (int u = 0; u < SPT; ++u) {
+            const unsigned g = genotype(bytes[u], s);
+            const R rec = clampr(hh[u], ELO, EHI);
             const R omr = (R)1 - rec;
             const R ga = (g == 3u) ? (R)0 : (R)g;
             const R gb = (g == 3u) ? (R)0 : (R)(2u - g);
@@ -192,41 +196,45 @@ em_sweep_kernel(const uint8_t* __restrict__ G, const R* __restrict__ P, const R*
             for (int k = 0; k < KMAX; ++k) tab[u][k] += d * Ps[jl][k];
             tb[u] += b[u];
           }
+          // this thread's part of value v of the SNP: A column v (v < KMAX), else B column
+          // v - KMAX, summed over its samples
+          auto part_of = [&](int v) {
+            R acc = 0;
+            if (v < KMAX) {
+#pragma unroll
+              for (int u = 0; u < SPT; ++u) acc += a[u] * q[u][v < KMAX ? v : 0];
+            } else if (v < V) {
+#pragma unroll
+              for (int u = 0; u < SPT; ++u) acc += b[u] * q[u][v >= KMAX && v < V ? v - KMAX : 0];
+            }
+            return acc;
+          };
           if constexpr (V <= 16) {
             // at most 16 values: a power-of-two vector of VR, reduced with fewer shuffles
             constexpr int VR = V <= 4 ? 4 : (V <= 8 ? 8 : 16);
             R part[VR];
 #pragma unroll
-            for (int v = 0; v < VR; ++v) {
-              R acc = 0;
-              if (v < KMAX) {
-#pragma unroll
-                for (int u = 0; u < SPT; ++u) acc += a[u] * q[u][v < KMAX ? v : 0];
-              } else if (v < V) {
-#pragma unroll
-                for (int u = 0; u < SPT; ++u) acc += b[u] * q[u][v >= KMAX && v < V ? v - KMAX : 0];
-              }
-              part[v] = acc;
-            }
+            for (int v = 0; v < VR; ++v) part[v] = part_of(v);
             // lanes >= VR hold copies of lanes & (VR - 1): slots V.. of red are never read
             red[warp][jl][lane] = reduce_scatter_small<VR>(part, lane);
+          } else if constexpr (V < 32 && ((V - 16) & (V - 17)) == 0) {
+            // 16 + 4 or 16 + 8 values: two power-of-two vectors, 16 + 6 or 16 + 9 shuffle
+            // steps instead of 31; lane l < 16 holds value l, lane 16 + i value 16 + i
+            constexpr int VR2 = V - 16;
+            R p1[16], p2[VR2];
+#pragma unroll
+            for (int v = 0; v < 16; ++v) p1[v] = part_of(v);
+#pragma unroll
+            for (int v = 0; v < VR2; ++v) p2[v] = part_of(16 + v);
+            const R r1 = reduce_scatter_small<16>(p1, lane);
+            const R r2 = reduce_scatter_small<VR2>(p2, lane);
+            red[warp][jl][lane] = lane < 16 ? r1 : r2;
           } else {
 #pragma unroll
             for (int c = 0; c < C::NCH; ++c) {
               R part[32];
 #pragma unroll
-              for (int l = 0; l < 32; ++l) {
-                const int v = c * 32 + l;
-                R acc = 0;
-                if (v < KMAX) {
-#pragma unroll
-                  for (int u = 0; u < SPT; ++u) acc += a[u] * q[u][v < KMAX ? v : 0];
-                } else if (v < V) {
-#pragma unroll
-                  for (int u = 0; u < SPT; ++u) acc += b[u] * q[u][v >= KMAX && v < V ? v - KMAX : 0];
-                }
-                part[l] = acc;
-              }
+              for (int l = 0; l < 32; ++l) part[l] = part_of(c * 32 + l);
               red[warp][jl][c * 32 + lane] = reduce_scatter32(part, lane);
             }
           }
