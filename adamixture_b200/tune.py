@@ -139,9 +139,9 @@ def tune_dmma(G: torch.Tensor, P: torch.Tensor, Q: torch.Tensor, M: int, workspa
         _load_cache()
         key = _key(dev, M, N, K)
         hit = _CACHE.get(key)
-        if hit is not None and not force:
-            set_tile(K, int(hit["tile"]), dev)
-            return int(hit["tile"])
+        if hit is not None and not force and isinstance(hit.get("tile"), int) and 0 <= hit["tile"] < n:
+            set_tile(K, hit["tile"], dev)
+            return hit["tile"]
         sms = torch.cuda.get_device_properties(dev).multi_processor_count
         nb = timed_blocks(M, N, K, sms)
         ws = workspace if workspace is not None else ops.em_workspace(M, N, K, "f64", G.device)

@@ -60,3 +60,26 @@ def test_autotune_switch(monkeypatch):
     assert not tune.enabled()
     monkeypatch.setenv("ADX_AUTOTUNE", "1")
     assert tune.enabled()
+
+
+def test_cache_file_round_trip(tmp_path, monkeypatch):
+    f = tmp_path / "sub" / "tune.json"
+    monkeypatch.setenv("ADX_TUNE_CACHE", str(f))
+    monkeypatch.setattr(tune, "_CACHE", {"B200|M=10|N=20|K=3": {"tile": 1, "ms": {"0": 2.0, "1": 1.5}, "blocks": 4}})
+    monkeypatch.setattr(tune, "_LOADED", True)
+    tune._save_cache()
+    assert f.exists()
+    monkeypatch.setattr(tune, "_CACHE", {})
+    monkeypatch.setattr(tune, "_LOADED", False)
+    tune._load_cache()
+    assert tune.choices() == {"B200|M=10|N=20|K=3": {"tile": 1, "ms": {"0": 2.0, "1": 1.5}, "blocks": 4}}
+
+
+def test_unreadable_cache_file_is_ignored(tmp_path, monkeypatch):
+    f = tmp_path / "tune.json"
+    f.write_text("{not json")
+    monkeypatch.setenv("ADX_TUNE_CACHE", str(f))
+    monkeypatch.setattr(tune, "_CACHE", {})
+    monkeypatch.setattr(tune, "_LOADED", False)
+    tune._load_cache()
+    assert tune.choices() == {}
