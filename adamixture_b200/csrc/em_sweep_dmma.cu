@@ -74,8 +74,8 @@ __device__ __forceinline__ int dsw(int r) { return ((r >> 3) & 3) << 2; }
 //   1 (K <= 8): Q rows of 16 doubles (8 columns, swizzled by Lay<1>::sw), P groups of 4
 //     chunks in rows of 12, 8 A/B values a thread; 112 KiB and at most 128 registers a
 //     thread, so two CTAs share an SM.
-// Both layouts' fragment loads and stores were checked exhaustively (every half-warp of
-// every access pattern) to be free of bank conflicts.
+// Both layouts' fragment loads and stores are checked exhaustively (every half-warp of every
+// access pattern: in bounds, free of bank conflicts) by tests/test_dmma_layouts_cpu.py.
 template <int TL> struct Lay;
 template <> struct Lay<0> {
   static constexpr int QSTR = 24, QC = 16, PSTR = 20, PC = 16, GRP = 8, NV = 16, OCC = 1, KSMAX = 4;
