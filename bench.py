@@ -1243,7 +1243,7 @@ def main():
     ap.add_argument("--cv-polish", dest="cv_polish", type=int, default=10,
                     help="c4: Adam-EM iterations per fold")
     ap.add_argument("--train", action="store_true", help="c5: train the warm-start network first")
-    ap.add_argument("--weights-out", dest="weights_out", default="gpurun_out/warm_start_weights.npz",
+    ap.add_argument("--weights-out", dest="weights_out", default="warm_start_weights.npz",
                     help="c5 --train: where the trained weights go")
     ap.add_argument("--batch-sweeps", dest="batch_sweeps", action="store_true",
                     help="c4: time single and batched sweep launches instead of the CV runs")
