@@ -47,12 +47,12 @@ class CudaInitBackend:
     def rsvd_cols(self, G, f, B, M_local):
         from .. import ops
 
-        return ops.rsvd_cols(G, f, B, M_local)
+        return ops.rsvd_cols(G, f.to(torch.float32).contiguous(), B, M_local)
 
     def rsvd_rows(self, G, f, Y, M_local):
         from .. import ops
 
-        return ops.rsvd_rows(G, f, Y, M_local)
+        return ops.rsvd_rows(G, f.to(torch.float32).contiguous(), Y, M_local)
 
     def bvls(self, A, B, lower, upper):
         from .. import ops
