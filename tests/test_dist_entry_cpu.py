@@ -123,3 +123,12 @@ def test_two_rank_run_matches_one_rank(tmp_path, algorithm):
     Pf = np.loadtxt(outs[2] / "run.3.P")
     np.testing.assert_allclose(Qf, r2["Q"], rtol=1e-15)
     np.testing.assert_allclose(Pf, r2["P"], rtol=1e-15)
+
+
+@pytest.mark.parametrize("bad", [["--k", "0"], ["--k", "65"], ["--k", "3", "--device", "cpu"],
+                                 ["--k", "3", "--lr", "-1"]])
+def test_bad_options_are_rejected(bad):
+    from adamixture_b200.dist_entry import parse_args
+
+    with pytest.raises(SystemExit):
+        parse_args(bad + ["--data_path", "x.bed", "--save_dir", "o", "--name", "r"])
